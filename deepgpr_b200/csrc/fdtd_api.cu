@@ -1,0 +1,998 @@
+// fdtd_api.cu -- C-ABI entry points of libdeepgpr_b200.so.
+//
+// ABI 6 of the reference (src/DeepGPR/lib/deepgpr.h:41-152) is exported
+// unchanged, so the reference's own ctypes bridge can load this library in
+// place of deepgpr.so.  The extensions (dgb_*) add an explicit CUDA stream,
+// FP64 instantiations, FP8 histories and launch options; see
+// include/deepgpr_b200.h for the full list.
+//
+// Execution model: one call = one time loop.  All work of a call runs on a
+// private stream of the calling thread that is ordered after (and before)
+// the caller's stream with events.  The time loop is issued in chunks of
+// `chunk` steps; a chunk is captured once into a CUDA graph and replayed.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "fdtd_tiled_adj.cuh"
+
+#define DGB_API extern "C" __attribute__((visibility("default")))
+
+namespace {
+
+using namespace dg;
+
+// storage_type bits (src/DeepGPR/config/constants.py:128-187)
+constexpr int ST_KIND_MASK = 0x0f;
+constexpr int ST_RHS_FROM_E = 1 << 4;
+constexpr int ST_PHYSICAL = 1 << 5;
+constexpr int ST_TM2D = 1 << 6;
+constexpr int ST_DISABLED = 1 << 26;
+
+thread_local char g_error[512];
+int g_order = 2;  // process-global like the reference (set_fdtd_order)
+
+struct ThreadOptions {
+  cudaStream_t user_stream = nullptr;  // nullptr: legacy default stream
+  bool user_stream_set = false;
+  int acc64 = 1;          // FP64 accumulation of the material gradient
+  int chunk = 16;         // time steps per launch chunk
+  int use_graph = 1;      // capture a chunk into a CUDA graph and replay it
+  int order_override = 0; // per-thread FDTD order (0: use the global)
+};
+thread_local ThreadOptions g_opt;
+
+void set_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_error, sizeof(g_error), fmt, ap);
+  va_end(ap);
+}
+
+bool cuda_ok(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return true;
+  set_error("%s: %s", what, cudaGetErrorString(e));
+  return false;
+}
+
+int radius_of(int order) { return order >= 8 ? 4 : (order >= 4 ? 2 : 1); }
+
+// Per-thread, per-device private stream and events.
+struct StreamSet {
+  int device = -1;
+  cudaStream_t work = nullptr;
+  cudaEvent_t in = nullptr, out = nullptr;
+};
+thread_local std::vector<StreamSet> g_streams;
+
+StreamSet* stream_set() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  for (auto& s : g_streams)
+    if (s.device == dev) return &s;
+  StreamSet s;
+  s.device = dev;
+  if (cudaStreamCreateWithFlags(&s.work, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
+  if (cudaEventCreateWithFlags(&s.in, cudaEventDisableTiming) != cudaSuccess) return nullptr;
+  if (cudaEventCreateWithFlags(&s.out, cudaEventDisableTiming) != cudaSuccess) return nullptr;
+  g_streams.push_back(s);
+  return &g_streams.back();
+}
+
+cudaStream_t caller_stream() { return g_opt.user_stream_set ? g_opt.user_stream : cudaStreamLegacy; }
+
+// Scratch owned by one call; released (stream-ordered) on destruction.
+struct Scratch {
+  cudaStream_t st;
+  std::vector<void*> blocks;
+  bool failed = false;
+  explicit Scratch(cudaStream_t s) : st(s) {}
+  template <typename P>
+  P* get(size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    void* p = nullptr;
+    cudaError_t e = cudaMallocAsync(&p, bytes, st);
+    if (e != cudaSuccess) {
+      set_error("cudaMallocAsync(%zu bytes): %s", bytes, cudaGetErrorString(e));
+      failed = true;
+      return nullptr;
+    }
+    blocks.push_back(p);
+    return static_cast<P*>(p);
+  }
+  ~Scratch() {
+    for (void* p : blocks) cudaFreeAsync(p, st);
+  }
+};
+
+// Sorted point table (see PointTable in fdtd_common.cuh) built on the host
+// from the caller's (nshot, npts, 3) int32 locations.
+bool build_table(const int* loc, int nshot, int npts, const Grid& g, cudaStream_t st, Scratch& scratch,
+                 PointTable* out, const char* what, int err_code) {
+  out->n = 0;
+  out->cells = out->off = out->shot = out->idx = nullptr;
+  if (npts <= 0 || nshot <= 0 || loc == nullptr) return true;
+  const size_t n = (size_t)nshot * npts;
+  std::vector<int> h(n * 3);
+  if (!cuda_ok(cudaMemcpyAsync(h.data(), loc, n * 3 * sizeof(int), cudaMemcpyDefault, st), what)) return false;
+  if (!cuda_ok(cudaStreamSynchronize(st), what)) return false;
+  struct E {
+    int cell, shot, idx;
+  };
+  std::vector<E> ent(n);
+  for (int s = 0; s < nshot; ++s)
+    for (int m = 0; m < npts; ++m) {
+      const int* p = &h[((size_t)s * npts + m) * 3];
+      if (p[0] < 0 || p[0] >= g.NX || p[1] < 0 || p[1] >= g.NY || p[2] < 0 || p[2] >= g.NZ) {
+        set_error("%s location (%d, %d, %d) of shot %d, index %d is outside the field grid (%d, %d, %d)", what,
+                  p[0], p[1], p[2], s, m, g.NX, g.NY, g.NZ);
+        (void)err_code;
+        return false;
+      }
+      ent[(size_t)s * npts + m] = E{p[0] * g.sx + p[1] * g.NZ + p[2], s, m};
+    }
+  std::sort(ent.begin(), ent.end(), [](const E& a, const E& b) {
+    if (a.cell != b.cell) return a.cell < b.cell;
+    if (a.shot != b.shot) return a.shot < b.shot;
+    return a.idx < b.idx;
+  });
+  std::vector<int> cells, off, shot(n), idx(n);
+  for (size_t e = 0; e < n; ++e) {
+    if (e == 0 || ent[e].cell != ent[e - 1].cell) {
+      cells.push_back(ent[e].cell);
+      off.push_back((int)e);
+    }
+    shot[e] = ent[e].shot;
+    idx[e] = ent[e].idx;
+  }
+  off.push_back((int)n);
+  const size_t U = cells.size();
+  std::vector<int> packed;
+  packed.reserve(U + (U + 1) + 2 * n);
+  packed.insert(packed.end(), cells.begin(), cells.end());
+  packed.insert(packed.end(), off.begin(), off.end());
+  packed.insert(packed.end(), shot.begin(), shot.end());
+  packed.insert(packed.end(), idx.begin(), idx.end());
+  int* d = scratch.get<int>(packed.size() * sizeof(int));
+  if (!d) return false;
+  if (!cuda_ok(cudaMemcpyAsync(d, packed.data(), packed.size() * sizeof(int), cudaMemcpyHostToDevice, st), what))
+    return false;
+  // the pageable source must stay valid until the copy ran
+  if (!cuda_ok(cudaStreamSynchronize(st), what)) return false;
+  out->cells = d;
+  out->off = d + U;
+  out->shot = d + U + (U + 1);
+  out->idx = d + U + (U + 1) + n;
+  out->n = (int)U;
+  return true;
+}
+
+// Table plus per-shot membership bitmaps.
+bool build_pointset(const int* loc, int nshot, int npts, const Grid& g, cudaStream_t st, Scratch& scratch,
+                    PointSet* ps, PointTable* tb_out, const char* what, int err_code) {
+  ps->tb.n = 0;
+  ps->tb.cells = ps->tb.off = ps->tb.shot = ps->tb.idx = nullptr;
+  ps->bits = nullptr;
+  ps->words_per_shot = (g.cells + 31) / 32;
+  if (!build_table(loc, nshot, npts, g, st, scratch, &ps->tb, what, err_code)) return false;
+  if (tb_out) *tb_out = ps->tb;
+  if (ps->tb.n == 0) return true;
+  // rebuild the bitmap on the host from the same (validated) locations
+  const size_t n = (size_t)nshot * npts;
+  std::vector<int> h(n * 3);
+  if (!cuda_ok(cudaMemcpyAsync(h.data(), loc, n * 3 * sizeof(int), cudaMemcpyDefault, st), what)) return false;
+  if (!cuda_ok(cudaStreamSynchronize(st), what)) return false;
+  std::vector<unsigned> bits((size_t)nshot * ps->words_per_shot, 0u);
+  for (int s = 0; s < nshot; ++s)
+    for (int m = 0; m < npts; ++m) {
+      const int* p = &h[((size_t)s * npts + m) * 3];
+      const int c = p[0] * g.sx + p[1] * g.NZ + p[2];
+      bits[(size_t)s * ps->words_per_shot + (c >> 5)] |= 1u << (c & 31);
+    }
+  unsigned* d = scratch.get<unsigned>(bits.size() * sizeof(unsigned));
+  if (!d) return false;
+  if (!cuda_ok(cudaMemcpyAsync(d, bits.data(), bits.size() * sizeof(unsigned), cudaMemcpyHostToDevice, st), what))
+    return false;
+  if (!cuda_ok(cudaStreamSynchronize(st), what)) return false;
+  ps->bits = d;
+  return true;
+}
+
+// x-chunk length that gives about 8 resident CTAs per SM.
+int pick_xchunk(int NX, long long tiles_per_plane, int nshot, int min_chunk) {
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long target = (long long)sms * 8;
+  const long long per = std::max<long long>(1, tiles_per_plane * nshot);
+  long long chunks = (target + per - 1) / per;
+  chunks = std::max<long long>(1, std::min<long long>(chunks, 65535));
+  int xc = (int)((NX + chunks - 1) / chunks);
+  xc = std::max(xc, std::min(min_chunk, NX));
+  return xc;
+}
+
+long long tiles3(const Grid& g) { return (long long)((g.NY + TY - 1) / TY) * ((g.NZ + TZ - 1) / TZ); }
+long long tiles2(const Grid& g) { return (long long)(g.NY + T2 - 1) / T2; }
+
+template <typename T>
+__global__ void k_coeffs(const T* __restrict__ eps, const T* __restrict__ sig, const T* __restrict__ mu,
+                         T* ce_hist, T* ce_curl, T* ce_rhs, T* ch_hist, T* ch_curl, T* ch_rhs, Grid g, T dt,
+                         T dx) {
+  // src/DeepGPR/lib/deepgpr_cpu.c:547-584; halo cells are set to zero.
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= g.cells) return;
+  int i, j, k;
+  cell_ijk(g, c, i, j, k);
+  if (i >= g.NX - 1 || j >= g.NY - 1 || k >= g.NZ - 1) {
+    ce_hist[c] = ce_curl[c] = ce_rhs[c] = ch_hist[c] = ch_curl[c] = ch_rhs[c] = T(0);
+    return;
+  }
+  const T m0 = sizeof(T) == 4 ? T(1.25663706212e-06f) : T(1.25663706212e-06);
+  const T e0 = Phys<T>::eps0();
+  const T ha = m0 * mu[c] / dt;
+  ch_hist[c] = T(1);
+  ch_curl[c] = (T(1) / dx) / ha;
+  ch_rhs[c] = T(1) / ha;
+  if (sig[c] > Phys<T>::pec()) {
+    ce_hist[c] = ce_curl[c] = ce_rhs[c] = T(0);
+  } else {
+    const T e = e0 * eps[c] / dt;
+    const T s = T(0.5) * sig[c];
+    const T a = e + s, b = e - s;
+    ce_hist[c] = b / a;
+    ce_curl[c] = (T(1) / dx) / a;
+    ce_rhs[c] = T(1) / a;
+  }
+}
+
+__global__ void k_advance(Control* ctrl, int delta) { ctrl->cur += delta; }
+
+__global__ void k_set(Control* ctrl, int cur) {
+  ctrl->cur = cur;
+  ctrl->error = 0;
+}
+
+HBox make_box(const Grid& g, bool physical, const int* p) {
+  HBox b;
+  if (physical) {
+    b.x0 = p[0];
+    b.y0 = p[2];
+    b.z0 = p[4];
+    b.nx = g.NX - 1 - p[0] - p[1];
+    b.ny = g.NY - 1 - p[2] - p[3];
+    b.nz = g.NZ - 1 - p[4] - p[5];
+  } else {
+    b.x0 = b.y0 = b.z0 = 0;
+    b.nx = g.NX - 1;
+    b.ny = g.NY - 1;
+    b.nz = g.NZ - 1;
+  }
+  return b;
+}
+
+long long ntiles_of(const Grid& g) { return ((long long)g.cells + kBlock - 1) / kBlock; }
+
+// FP8 scale tiles: one per (x plane, CTA tile) of the forward kernels.
+long long fp8_tiles(const Grid& g, bool tm2d) {
+  return (long long)g.NX * (tm2d ? (long long)(g.NY + T2 - 1) / T2
+                                 : (long long)((g.NY + TY - 1) / TY) * ((g.NZ + TZ - 1) / TZ));
+}
+
+// FP8 history buffer: payload (1 byte per value) padded to 256 bytes, then
+// one float scale per (comp, slot, shot, tile).
+long long fp8_payload_bytes(long long values) { return (values + 255) / 256 * 256; }
+
+template <typename T>
+struct Common {
+  Grid g;
+  T dx, dy, dz, dt;
+  int nt, p[6];
+  const T *eps, *sig, *mu;
+  T *ce_hist, *ce_curl, *ce_rhs, *ch_hist, *ch_curl, *ch_rhs;
+  const T* eR[6];
+  const T* hR[6];
+  T* ePsi[12];
+  T* hPsi[12];
+  int S, mode, storage_type;
+};
+
+template <typename T>
+void fill_faces(Face<T>* F, const int* p, const T* const* R, T* const* psi) {
+  for (int f = 0; f < 6; ++f) {
+    F[f].R = R[f];
+    F[f].psi1 = psi[2 * f];
+    F[f].psi2 = psi[2 * f + 1];
+    F[f].w1 = F[f].w2 = nullptr;
+    F[f].p = p[f];
+  }
+}
+
+template <typename T>
+bool launch_coeffs(const Common<T>& cm, cudaStream_t st) {
+  const int blocks = (cm.g.cells + 255) / 256;
+  k_coeffs<T><<<blocks, 256, 0, st>>>(cm.eps, cm.sig, cm.mu, cm.ce_hist, cm.ce_curl, cm.ce_rhs, cm.ch_hist,
+                                      cm.ch_curl, cm.ch_rhs, cm.g, cm.dt, cm.dx);
+  return cuda_ok(cudaGetLastError(), "coefficient kernel");
+}
+
+// Issue `steps` time steps through `issue(k)` in chunks, with graph replay.
+template <typename Issue>
+bool run_loop(int steps, int dir, Control* ctrl, cudaStream_t st, Issue issue) {
+  const int chunk = std::max(1, g_opt.chunk);
+  cudaGraphExec_t exec = nullptr;
+  bool ok = true;
+  int t = 0;
+  while (ok && t < steps) {
+    const int K = std::min(chunk, steps - t);
+    if (g_opt.use_graph && K == chunk && steps >= 2 * chunk) {
+      if (!exec) {
+        cudaGraph_t graph = nullptr;
+        ok = cuda_ok(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
+        if (!ok) break;
+        for (int k = 0; k < K; ++k) issue(k);
+        k_advance<<<1, 1, 0, st>>>(ctrl, dir * K);
+        cudaError_t e1 = cudaGetLastError();
+        cudaError_t e2 = cudaStreamEndCapture(st, &graph);
+        ok = cuda_ok(e1, "capture launch") && cuda_ok(e2, "end capture");
+        if (!ok) break;
+        ok = cuda_ok(cudaGraphInstantiate(&exec, graph, 0), "graph instantiate");
+        cudaGraphDestroy(graph);
+        if (!ok) break;
+      }
+      ok = cuda_ok(cudaGraphLaunch(exec, st), "graph launch");
+    } else {
+      for (int k = 0; k < K; ++k) issue(k);
+      k_advance<<<1, 1, 0, st>>>(ctrl, dir * K);
+      ok = cuda_ok(cudaGetLastError(), "time-step launch");
+    }
+    t += K;
+  }
+  if (exec) cudaGraphExecDestroy(exec);
+  return ok;
+}
+
+template <typename T>
+struct ForwardCall {
+  Common<T> cm;
+  void *E_saved, *R_saved;
+  T *Ex, *Ey, *Ez, *Hx, *Hy, *Hz;
+  int nrx;
+  const int* rx_loc;
+  T* rx;
+  int rx_comp;
+  int nsrc;
+  const int* src_loc;
+  const T* wave;
+  int src_comp;
+  int save_model_history;
+};
+
+template <typename T>
+void forward_impl(const ForwardCall<T>& fc) {
+  g_error[0] = '\0';
+  const Common<T>& cm = fc.cm;
+  const Grid& g = cm.g;
+  if (g.NX < 2 || g.NY < 2 || g.NZ < 2 || g.nshot < 1 || cm.nt < 0) {
+    set_error("forward: invalid grid (%d, %d, %d), nshot %d, nt %d", g.NX, g.NY, g.NZ, g.nshot, cm.nt);
+    return;
+  }
+  if ((long long)g.NX * g.NY * g.NZ > 0x7fffffffLL) {
+    set_error("forward: %d x %d x %d field cells per shot exceed the 2^31 limit", g.NX, g.NY, g.NZ);
+    return;
+  }
+  if (cm.S < 1) {
+    set_error("forward: sampling interval must be positive");
+    return;
+  }
+  const int kind = cm.storage_type & ST_KIND_MASK;
+  const bool history = (cm.storage_type & ST_DISABLED) == 0;
+  const bool e_only = history && fc.save_model_history && (cm.storage_type & ST_RHS_FROM_E);
+  const bool keep_r = history && fc.save_model_history && !e_only;
+  const bool physical = (cm.storage_type & ST_PHYSICAL) != 0;
+  const bool tm2d = (cm.storage_type & ST_TM2D) != 0;
+  const bool has_cpml = cm.p[0] || cm.p[1] || cm.p[2] || cm.p[3] || cm.p[4] || cm.p[5];
+  if (history && fc.save_model_history && has_cpml && physical) {
+    set_error("forward: material gradients with PML require extended wavefield history; "
+              "physical history omits PML material sensitivities");
+    return;
+  }
+  if (e_only && cm.S != 1) {
+    set_error("forward: E-only wavefield history requires sampling interval 1");
+    return;
+  }
+  if (history && kind != kF32 && kind != kF16 && kind != kBF16 && kind != kFP8 && kind != kF64) {
+    set_error("forward: unsupported history storage kind %d", kind);
+    return;
+  }
+  if (history && kind == kFP8 && e_only) {
+    set_error("forward: FP8 histories keep E and R (E-only reconstruction is not supported for FP8)");
+    return;
+  }
+  if (history && (kind == kF64) != (sizeof(T) == 8)) {
+    set_error("forward: FP64 histories are used exactly by the FP64 entry points");
+    return;
+  }
+  if (tm2d && (g.NZ != 2 || fc.src_comp != 2 || (history && cm.mode != 2))) {
+    set_error("forward: the 2D TM path needs nz = 1, an Ez source and gradient mode 2");
+    return;
+  }
+  StreamSet* ss = stream_set();
+  if (!ss) {
+    set_error("forward: cannot create the CUDA stream");
+    return;
+  }
+  const cudaStream_t user = caller_stream();
+  const cudaStream_t st = ss->work;
+  if (!cuda_ok(cudaEventRecord(ss->in, user), "event record") || !cuda_ok(cudaStreamWaitEvent(st, ss->in, 0), "wait"))
+    return;
+  bool ok = true;
+  {
+    Scratch scratch(st);
+    TiledFwd<T> P;
+    memset(&P, 0, sizeof(P));
+    FwdArgs<T>& a = P.a;
+    a.g = g;
+    a.dx = cm.dx;
+    a.dy = cm.dy;
+    a.dz = cm.dz;
+    a.dy_eq = cm.dy == cm.dx;
+    a.dz_eq = cm.dz == cm.dx;
+    a.Ex = fc.Ex; a.Ey = fc.Ey; a.Ez = fc.Ez;
+    a.Hx = fc.Hx; a.Hy = fc.Hy; a.Hz = fc.Hz;
+    a.ce_hist = cm.ce_hist;
+    a.ce_curl = cm.ce_curl;
+    a.ce_rhs = cm.ce_rhs;
+    a.ch_curl = cm.ch_curl;
+    a.ch_rhs = cm.ch_rhs;
+    fill_faces(a.eF, cm.p, cm.eR, cm.ePsi);
+    fill_faces(a.hF, cm.p, cm.hR, cm.hPsi);
+    a.has_cpml = has_cpml;
+    a.nt = cm.nt;
+    a.wave = fc.wave;
+    a.src_comp = fc.src_comp;
+    a.src_dl = fc.src_comp == 0 ? cm.dx : (fc.src_comp == 1 ? cm.dy : cm.dz);
+    a.src_vol = cm.dx * cm.dy * cm.dz;
+    a.rx = fc.rx;
+    a.rx_comp = (fc.rx_comp < 0 || fc.rx_comp > 2) ? 2 : fc.rx_comp;  // deepgpr_cpu.c:620
+    a.nrx = fc.nrx;
+    a.save_e = history;
+    a.keep_r = keep_r;
+    a.S = cm.S;
+    a.mode = cm.mode;
+    a.kind = kind;
+    a.nt_saved = (cm.nt + cm.S - 1) / cm.S;
+    a.box = make_box(g, physical, cm.p);
+    a.frame = (long long)g.nshot * a.box.cells();
+    a.comp_stride = (long long)a.nt_saved * a.frame;
+    a.E_saved = fc.E_saved;
+    a.R_saved = fc.R_saved;
+    a.ntiles = (int)fp8_tiles(g, tm2d);
+    const int ncomp = cm.mode == 3 ? 3 : 1;
+    if (history && kind == kFP8) {
+      const long long vals = (long long)ncomp * a.comp_stride;
+      a.e_scales = reinterpret_cast<float*>(static_cast<char*>(fc.E_saved) + fp8_payload_bytes(vals));
+      if (keep_r) a.r_scales = reinterpret_cast<float*>(static_cast<char*>(fc.R_saved) + fp8_payload_bytes(vals));
+    }
+    Control* ctrl = scratch.get<Control>(sizeof(Control));
+    ok = !scratch.failed;
+    // sources of an invalid component inject nothing (deepgpr_cpu.c:650)
+    if (ok && fc.src_comp >= 0 && fc.src_comp <= 2)
+      ok = build_pointset(fc.src_loc, g.nshot, fc.nsrc, g, st, scratch, &P.src, &a.src, "source", kErrSourceRange);
+    if (ok) ok = build_pointset(fc.rx_loc, g.nshot, fc.nrx, g, st, scratch, &P.rcv, &a.rcv, "receiver", kErrReceiverRange);
+    if (ok) ok = launch_coeffs(cm, st);
+    TmFields<T> tf;
+    memset(&tf, 0, sizeof(tf));
+    const long long plane2 = (long long)g.NX * g.NY;
+    if (ok && tm2d) {
+      T* buf = scratch.get<T>((size_t)(3 * g.nshot + 5) * plane2 * sizeof(T));
+      ok = buf != nullptr;
+      if (ok) {
+        tf.Ez = buf;
+        tf.Hx = buf + g.nshot * plane2;
+        tf.Hy = buf + 2 * g.nshot * plane2;
+        T* cf = buf + 3 * g.nshot * plane2;
+        const T* srcs[5] = {cm.ce_hist, cm.ce_curl, cm.ce_rhs, cm.ch_curl, cm.ch_rhs};
+        for (int q = 0; q < 5; ++q) k_pack2d<T><<<1024, 256, 0, st>>>(srcs[q], cf + q * plane2, plane2);
+        tf.ce_hist = cf;
+        tf.ce_curl = cf + plane2;
+        tf.ce_rhs = cf + 2 * plane2;
+        tf.ch_curl = cf + 3 * plane2;
+        tf.ch_rhs = cf + 4 * plane2;
+        k_pack2d<T><<<2048, 256, 0, st>>>(fc.Ez, tf.Ez, g.nshot * plane2);
+        k_pack2d<T><<<2048, 256, 0, st>>>(fc.Hx, tf.Hx, g.nshot * plane2);
+        k_pack2d<T><<<2048, 256, 0, st>>>(fc.Hy, tf.Hy, g.nshot * plane2);
+        ok = cuda_ok(cudaGetLastError(), "pack");
+      }
+    }
+    if (ok) {
+      a.ctrl = ctrl;
+      k_set<<<1, 1, 0, st>>>(ctrl, 0);
+      const int R = radius_of(g_opt.order_override ? g_opt.order_override : g_order);
+      const long long tiles = tm2d ? tiles2(g) : tiles3(g);
+      P.xchunk = pick_xchunk(g.NX, tiles, g.nshot, 4 * R);
+      P.tm2d = tm2d;
+      dim3 grid((unsigned)tiles, (unsigned)((g.NX + P.xchunk - 1) / P.xchunk), (unsigned)g.nshot);
+      auto issue = [&](int k) {
+        TiledFwd<T> b = P;
+        b.a.k_in_chunk = k;
+        if (tm2d) {
+          if (R == 1) { k2_fwd_h<T, 1><<<grid, T2, 0, st>>>(b, tf); k2_fwd_e<T, 1><<<grid, T2, 0, st>>>(b, tf); }
+          else if (R == 2) { k2_fwd_h<T, 2><<<grid, T2, 0, st>>>(b, tf); k2_fwd_e<T, 2><<<grid, T2, 0, st>>>(b, tf); }
+          else { k2_fwd_h<T, 4><<<grid, T2, 0, st>>>(b, tf); k2_fwd_e<T, 4><<<grid, T2, 0, st>>>(b, tf); }
+        } else {
+          if (R == 1) { k3_fwd_h<T, 1><<<grid, 256, 0, st>>>(b); k3_fwd_e<T, 1><<<grid, 256, 0, st>>>(b); }
+          else if (R == 2) { k3_fwd_h<T, 2><<<grid, 256, 0, st>>>(b); k3_fwd_e<T, 2><<<grid, 256, 0, st>>>(b); }
+          else { k3_fwd_h<T, 4><<<grid, 256, 0, st>>>(b); k3_fwd_e<T, 4><<<grid, 256, 0, st>>>(b); }
+        }
+      };
+      ok = run_loop(cm.nt, +1, ctrl, st, issue);
+      if (ok && tm2d) {
+        k_unpack2d<T><<<2048, 256, 0, st>>>(tf.Ez, fc.Ez, g.nshot * plane2);
+        k_unpack2d<T><<<2048, 256, 0, st>>>(tf.Hx, fc.Hx, g.nshot * plane2);
+        k_unpack2d<T><<<2048, 256, 0, st>>>(tf.Hy, fc.Hy, g.nshot * plane2);
+        ok = cuda_ok(cudaGetLastError(), "unpack");
+      }
+      if (ok && e_only) {
+        // closing E^nt frame into R_saved (deepgpr_cpu.c:1919-1930)
+        const long long bc = a.box.cells();
+        for (int q = 0; q < ncomp; ++q) {
+          const int fcmp = cm.mode == 3 ? q : 2;
+          const T* E = fcmp == 0 ? fc.Ex : (fcmp == 1 ? fc.Ey : fc.Ez);
+          void* dst = static_cast<char*>(fc.R_saved) + (long long)q * g.nshot * bc * hist_elem_bytes(kind);
+          k_final_frame<T><<<512, 256, 0, st>>>(E, dst, g, a.box, kind);
+        }
+        ok = cuda_ok(cudaGetLastError(), "final frame");
+      }
+    }
+  }
+  cudaEventRecord(ss->out, st);
+  cudaStreamWaitEvent(user, ss->out, 0);
+  if (ok) cuda_ok(cudaGetLastError(), "forward");
+}
+
+
+template <typename T>
+struct BackwardCall {
+  Common<T> cm;
+  const void *E_saved, *R_saved;
+  T *lEx, *lEy, *lEz, *lHx, *lHy, *lHz;
+  int ndata;
+  const int* rx_loc;
+  const T* data_grad;
+  int rx_comp;
+  int nsrc;
+  const int* src_loc;
+  int src_comp;
+  T* grad_source;
+  int want_src;
+  T *grad_eps, *grad_sig;
+  int want_eps, want_sig;
+};
+
+// Element counts of the 12 psi arrays of one field (E or H), in the order
+// x0 psi1, x0 psi2, xm psi1, ..., zm psi2.
+template <bool EFIELD>
+void psi_counts(const Grid& g, const int* p, long long* out) {
+  for (int f = 0; f < 6; ++f) {
+    const int axis = f / 2, q = p[f];
+    for (int slot = 1; slot <= 2; ++slot) {
+      long long a, b, c;
+      const int pe = EFIELD ? q + 1 : q;
+      if (axis == 0) {
+        a = pe;
+        b = slot == 1 ? (EFIELD ? g.NY - 1 : g.NY) : (EFIELD ? g.NY : g.NY - 1);
+        c = slot == 1 ? (EFIELD ? g.NZ : g.NZ - 1) : (EFIELD ? g.NZ - 1 : g.NZ);
+      } else if (axis == 1) {
+        a = slot == 1 ? (EFIELD ? g.NX - 1 : g.NX) : (EFIELD ? g.NX : g.NX - 1);
+        b = pe;
+        c = slot == 1 ? (EFIELD ? g.NZ : g.NZ - 1) : (EFIELD ? g.NZ - 1 : g.NZ);
+      } else {
+        a = slot == 1 ? (EFIELD ? g.NX - 1 : g.NX) : (EFIELD ? g.NX : g.NX - 1);
+        b = slot == 1 ? (EFIELD ? g.NY : g.NY - 1) : (EFIELD ? g.NY - 1 : g.NY);
+        c = pe;
+      }
+      out[2 * f + slot - 1] = q > 0 ? (long long)g.nshot * a * b * c : 0;
+    }
+  }
+}
+
+template <typename T>
+void backward_impl(const BackwardCall<T>& bc) {
+  g_error[0] = '\0';
+  const Common<T>& cm = bc.cm;
+  const Grid& g = cm.g;
+  if (g.NX < 2 || g.NY < 2 || g.NZ < 2 || g.nshot < 1 || cm.nt < 0 || cm.S < 1) {
+    set_error("backward: invalid grid (%d, %d, %d), nshot %d, nt %d, interval %d", g.NX, g.NY, g.NZ, g.nshot,
+              cm.nt, cm.S);
+    return;
+  }
+  if ((long long)g.NX * g.NY * g.NZ > 0x7fffffffLL) {
+    set_error("backward: %d x %d x %d field cells per shot exceed the 2^31 limit", g.NX, g.NY, g.NZ);
+    return;
+  }
+  const int kind = cm.storage_type & ST_KIND_MASK;
+  const bool want_model = bc.want_eps || bc.want_sig;
+  const bool e_only = want_model && (cm.storage_type & ST_RHS_FROM_E);
+  const bool physical = (cm.storage_type & ST_PHYSICAL) != 0;
+  const bool tm2d = (cm.storage_type & ST_TM2D) != 0;
+  const bool has_cpml = cm.p[0] || cm.p[1] || cm.p[2] || cm.p[3] || cm.p[4] || cm.p[5];
+  if (want_model && has_cpml && physical) {
+    set_error("backward: material gradients with PML require extended wavefield history; "
+              "physical history omits PML material sensitivities");
+    return;
+  }
+  if (e_only && cm.S != 1) {
+    set_error("backward: E-only wavefield history requires sampling interval 1");
+    return;
+  }
+  if (want_model && kind == kFP8 && e_only) {
+    set_error("backward: FP8 histories keep E and R (E-only reconstruction is not supported for FP8)");
+    return;
+  }
+  if (want_model && (kind == kF64) != (sizeof(T) == 8)) {
+    set_error("backward: FP64 histories are used exactly by the FP64 entry points");
+    return;
+  }
+  if (tm2d && (g.NZ != 2 || bc.src_comp != 2 || (want_model && cm.mode != 2))) {
+    set_error("backward: the 2D TM path needs nz = 1, an Ez source and gradient mode 2");
+    return;
+  }
+  StreamSet* ss = stream_set();
+  if (!ss) {
+    set_error("backward: cannot create the CUDA stream");
+    return;
+  }
+  const cudaStream_t user = caller_stream();
+  const cudaStream_t st = ss->work;
+  if (!cuda_ok(cudaEventRecord(ss->in, user), "event record") || !cuda_ok(cudaStreamWaitEvent(st, ss->in, 0), "wait"))
+    return;
+  bool ok = true;
+  {
+    Scratch scratch(st);
+    TiledAdj<T> P;
+    memset(&P, 0, sizeof(P));
+    AdjArgs<T>& a = P.a;
+    a.g = g;
+    a.dx = cm.dx;
+    a.dy = cm.dy;
+    a.dz = cm.dz;
+    a.inv_dx = T(1) / cm.dx;
+    a.inv_dy = T(1) / cm.dy;
+    a.inv_dz = T(1) / cm.dz;
+    a.dy_eq = cm.dy == cm.dx;
+    a.dz_eq = cm.dz == cm.dx;
+    a.lEx = bc.lEx; a.lEy = bc.lEy; a.lEz = bc.lEz;
+    a.lHx = bc.lHx; a.lHy = bc.lHy; a.lHz = bc.lHz;
+    a.ce_hist = cm.ce_hist;
+    a.ce_curl = cm.ce_curl;
+    a.ce_rhs = cm.ce_rhs;
+    a.ch_curl = cm.ch_curl;
+    a.ch_rhs = cm.ch_rhs;
+    fill_faces(a.eF, cm.p, cm.eR, cm.ePsi);
+    fill_faces(a.hF, cm.p, cm.hR, cm.hPsi);
+    a.has_cpml = has_cpml;
+    a.nt = cm.nt;
+    a.data_grad = bc.data_grad;
+    a.rx_comp = bc.rx_comp;
+    a.nrx = bc.ndata;
+    a.want_src = bc.want_src == 1 && bc.src_comp >= 0 && bc.src_comp <= 2 && bc.nsrc > 0;
+    a.nsrc = bc.nsrc;
+    a.src_comp = bc.src_comp;
+    a.grad_source = bc.grad_source;
+    {
+      const T dl = bc.src_comp == 0 ? cm.dx : (bc.src_comp == 1 ? cm.dy : cm.dz);
+      a.src_geo = dl / (cm.dx * cm.dy * cm.dz);
+    }
+    a.want_eps = bc.want_eps == 1;
+    a.want_sig = bc.want_sig == 1;
+    a.acc64 = (sizeof(T) == 8) ? 1 : g_opt.acc64;
+    a.g_eps = bc.grad_eps;
+    a.g_sig = bc.grad_sig;
+    a.sigma = cm.sig;
+    a.dt = cm.dt;
+    a.S = cm.S;
+    a.mode = cm.mode;
+    a.kind = kind;
+    a.e_only = e_only;
+    a.nt_saved = (cm.nt + cm.S - 1) / cm.S;
+    a.box = make_box(g, physical, cm.p);
+    a.frame = (long long)g.nshot * a.box.cells();
+    a.comp_stride = (long long)a.nt_saved * a.frame;
+    a.E_saved = bc.E_saved;
+    a.R_saved = bc.R_saved;
+    a.ntiles = (int)fp8_tiles(g, tm2d);
+    const int ncomp = cm.mode == 3 ? 3 : 1;
+    if (want_model && kind == kFP8) {
+      const long long vals = (long long)ncomp * a.comp_stride;
+      a.e_scales = reinterpret_cast<const float*>(static_cast<const char*>(bc.E_saved) + fp8_payload_bytes(vals));
+      a.r_scales = reinterpret_cast<const float*>(static_cast<const char*>(bc.R_saved) + fp8_payload_bytes(vals));
+    }
+    Control* ctrl = scratch.get<Control>(sizeof(Control));
+    ok = !scratch.failed;
+    // CPML weight scratch, shaped like the psi arrays
+    if (ok && has_cpml) {
+      long long ce[12], ch[12], tot = 0;
+      psi_counts<true>(g, cm.p, ce);
+      psi_counts<false>(g, cm.p, ch);
+      for (int q = 0; q < 12; ++q) tot += ce[q] + ch[q];
+      T* w = scratch.get<T>((size_t)tot * sizeof(T));
+      ok = w != nullptr;
+      if (ok) {
+        cudaMemsetAsync(w, 0, (size_t)tot * sizeof(T), st);
+        long long o = 0;
+        for (int f = 0; f < 6; ++f) {
+          a.eF[f].w1 = w + o; o += ce[2 * f];
+          a.eF[f].w2 = w + o; o += ce[2 * f + 1];
+        }
+        for (int f = 0; f < 6; ++f) {
+          a.hF[f].w1 = w + o; o += ch[2 * f];
+          a.hF[f].w2 = w + o; o += ch[2 * f + 1];
+        }
+      }
+    }
+    if (ok && a.want_src) {
+      a.srcv = scratch.get<T>((size_t)g.nshot * bc.nsrc * sizeof(T));
+      ok = a.srcv != nullptr;
+      if (ok) cudaMemsetAsync(a.srcv, 0, (size_t)g.nshot * bc.nsrc * sizeof(T), st);
+      if (ok) ok = build_pointset(bc.src_loc, g.nshot, bc.nsrc, g, st, scratch, &P.src, &a.src, "source", kErrSourceRange);
+    }
+    if (ok && bc.rx_comp >= 0 && bc.rx_comp <= 2)
+      ok = build_pointset(bc.rx_loc, g.nshot, bc.ndata, g, st, scratch, &P.rcv, &a.rcv, "receiver", kErrReceiverRange);
+    const long long ncell_ext = (long long)(g.NX - 1) * (g.NY - 1) * (g.NZ - 1);
+    if (ok && want_model && a.acc64) {
+      a.g_eps64 = scratch.get<double>((size_t)ncell_ext * sizeof(double));
+      a.g_sig64 = scratch.get<double>((size_t)ncell_ext * sizeof(double));
+      ok = !scratch.failed;
+      if (ok) {
+        cudaMemsetAsync(a.g_eps64, 0, (size_t)ncell_ext * sizeof(double), st);
+        cudaMemsetAsync(a.g_sig64, 0, (size_t)ncell_ext * sizeof(double), st);
+      }
+    }
+    if (ok) ok = launch_coeffs(cm, st);
+    TmAdj<T> tl;
+    memset(&tl, 0, sizeof(tl));
+    const long long plane2 = (long long)g.NX * g.NY;
+    if (ok && tm2d) {
+      T* buf = scratch.get<T>((size_t)(3 * g.nshot + 5) * plane2 * sizeof(T));
+      ok = buf != nullptr;
+      if (ok) {
+        tl.lEz = buf;
+        tl.lHx = buf + g.nshot * plane2;
+        tl.lHy = buf + 2 * g.nshot * plane2;
+        T* cf = buf + 3 * g.nshot * plane2;
+        const T* srcs[5] = {cm.ce_hist, cm.ce_curl, cm.ce_rhs, cm.ch_curl, cm.ch_rhs};
+        for (int q = 0; q < 5; ++q) k_pack2d<T><<<1024, 256, 0, st>>>(srcs[q], cf + q * plane2, plane2);
+        tl.ce_hist = cf;
+        tl.ce_curl = cf + plane2;
+        tl.ce_rhs = cf + 2 * plane2;
+        tl.ch_curl = cf + 3 * plane2;
+        tl.ch_rhs = cf + 4 * plane2;
+        k_pack2d<T><<<2048, 256, 0, st>>>(bc.lEz, tl.lEz, g.nshot * plane2);
+        k_pack2d<T><<<2048, 256, 0, st>>>(bc.lHx, tl.lHx, g.nshot * plane2);
+        k_pack2d<T><<<2048, 256, 0, st>>>(bc.lHy, tl.lHy, g.nshot * plane2);
+        ok = cuda_ok(cudaGetLastError(), "pack");
+      }
+    }
+    if (ok && cm.nt > 0) {
+      a.ctrl = ctrl;
+      k_set<<<1, 1, 0, st>>>(ctrl, cm.nt - 1);
+      const int R = radius_of(g_opt.order_override ? g_opt.order_override : g_order);
+      const long long tiles = tm2d ? tiles2(g) : tiles3(g);
+      P.xchunk = pick_xchunk(g.NX, tiles, g.nshot, 4 * R);
+      dim3 grid((unsigned)tiles, (unsigned)((g.NX + P.xchunk - 1) / P.xchunk), (unsigned)g.nshot);
+      const unsigned img_blocks = (unsigned)((a.box.cells() + 255) / 256);
+      const T* lamx = tm2d ? tl.lEz : bc.lEx;
+      const T* lamy = tm2d ? tl.lEz : bc.lEy;
+      const T* lamz = tm2d ? tl.lEz : bc.lEz;
+      // head of step nt-1
+      {
+        TiledAdj<T> b = P;
+        b.a.k_in_chunk = 0;
+        if (tm2d) {
+          if (R == 1) k2_adj_h<T, 1, true><<<grid, T2, 0, st>>>(b, tl);
+          else if (R == 2) k2_adj_h<T, 2, true><<<grid, T2, 0, st>>>(b, tl);
+          else k2_adj_h<T, 4, true><<<grid, T2, 0, st>>>(b, tl);
+        } else {
+          if (R == 1) k3_adj_h<T, 1, true><<<grid, 256, 0, st>>>(b);
+          else if (R == 2) k3_adj_h<T, 2, true><<<grid, 256, 0, st>>>(b);
+          else k3_adj_h<T, 4, true><<<grid, 256, 0, st>>>(b);
+        }
+        ok = cuda_ok(cudaGetLastError(), "adjoint prologue");
+      }
+      auto issue = [&](int k) {
+        TiledAdj<T> b = P;
+        b.a.k_in_chunk = k;
+        if (want_model && img_blocks > 0) k_image<T><<<img_blocks, 256, 0, st>>>(b.a, lamx, lamy, lamz, tm2d ? 1 : 0);
+        if (tm2d) {
+          if (R == 1) { k2_adj_e<T, 1><<<grid, T2, 0, st>>>(b, tl); k2_adj_h<T, 1, false><<<grid, T2, 0, st>>>(b, tl); }
+          else if (R == 2) { k2_adj_e<T, 2><<<grid, T2, 0, st>>>(b, tl); k2_adj_h<T, 2, false><<<grid, T2, 0, st>>>(b, tl); }
+          else { k2_adj_e<T, 4><<<grid, T2, 0, st>>>(b, tl); k2_adj_h<T, 4, false><<<grid, T2, 0, st>>>(b, tl); }
+        } else {
+          if (R == 1) { k3_adj_e<T, 1><<<grid, 256, 0, st>>>(b); k3_adj_h<T, 1, false><<<grid, 256, 0, st>>>(b); }
+          else if (R == 2) { k3_adj_e<T, 2><<<grid, 256, 0, st>>>(b); k3_adj_h<T, 2, false><<<grid, 256, 0, st>>>(b); }
+          else { k3_adj_e<T, 4><<<grid, 256, 0, st>>>(b); k3_adj_h<T, 4, false><<<grid, 256, 0, st>>>(b); }
+        }
+      };
+      if (ok) ok = run_loop(cm.nt, -1, ctrl, st, issue);
+      if (ok && tm2d) {
+        k_unpack2d<T><<<2048, 256, 0, st>>>(tl.lEz, bc.lEz, g.nshot * plane2);
+        k_unpack2d<T><<<2048, 256, 0, st>>>(tl.lHx, bc.lHx, g.nshot * plane2);
+        k_unpack2d<T><<<2048, 256, 0, st>>>(tl.lHy, bc.lHy, g.nshot * plane2);
+        ok = cuda_ok(cudaGetLastError(), "unpack");
+      }
+      if (ok && want_model && a.acc64) {
+        if (a.want_eps) k_fold_acc64<T><<<1024, 256, 0, st>>>(bc.grad_eps, a.g_eps64, ncell_ext);
+        if (a.want_sig) k_fold_acc64<T><<<1024, 256, 0, st>>>(bc.grad_sig, a.g_sig64, ncell_ext);
+        ok = cuda_ok(cudaGetLastError(), "gradient fold");
+      }
+    }
+  }
+  cudaEventRecord(ss->out, st);
+  cudaStreamWaitEvent(user, ss->out, 0);
+  if (ok) cuda_ok(cudaGetLastError(), "backward");
+}
+
+
+Grid make_grid(int NX, int NY, int NZ, int nshot) {
+  Grid g;
+  g.NX = NX;
+  g.NY = NY;
+  g.NZ = NZ;
+  g.sx = NY * NZ;
+  g.cells = NX * NY * NZ;
+  g.nshot = nshot;
+  // Split shots over gridDim.y only when one shot does not fill the GPU.
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long target = (long long)sms * 8 * kBlock;  // threads for a full machine
+  int groups = 1;
+  if (g.cells > 0 && (long long)g.cells < target) groups = (int)std::min<long long>(nshot, target / g.cells + 1);
+  groups = std::max(1, std::min(groups, kMaxShotGroups));
+  g.shots_per_group = (nshot + groups - 1) / groups;
+  return g;
+}
+
+}  // namespace
+
+// ===========================================================================
+// Exported symbols.
+// ===========================================================================
+
+// Parameter lists shared by the FP32 ABI-6 entry points and the FP64
+// extensions (src/DeepGPR/lib/deepgpr.h:89-152, same order and meaning).
+#define DGB_FWD_PARAMS(T)                                                                                       \
+  const T *eps_r_pad, const T *sigma_pad, const T *mu_r_pad, void *E_saved, void *R_saved, T *Ex, T *Ey,       \
+      T *Ez, T *Hx, T *Hy, T *Hz, T *ce_hist, T *ce_curl, T *ce_rhs, T *ch_hist, T *ch_curl, T *ch_rhs,        \
+      T *x0e1, T *x0e2, T *x0h1, T *x0h2, T *xme1, T *xme2, T *xmh1, T *xmh2, T *y0e1, T *y0e2, T *y0h1,       \
+      T *y0h2, T *yme1, T *yme2, T *ymh1, T *ymh2, T *z0e1, T *z0e2, T *z0h1, T *z0h2, T *zme1, T *zme2,       \
+      T *zmh1, T *zmh2, int p0, int p1, int p2, int p3, int p4, int p5, const T *x0E, const T *xmE,           \
+      const T *y0E, const T *ymE, const T *z0E, const T *zmE, const T *x0H, const T *xmH, const T *y0H,      \
+      const T *ymH, const T *z0H, const T *zmH, T dt, int nt, int nshot, int nrx, T dx, T dy, T dz,           \
+      const int *rx_loc, T *rx_out, int rx_comp, int NX, int NY, int NZ, int nsrc, const int *src_loc,        \
+      const T *src_wave, int src_comp, int S, int mode, int storage_type, int save_model_history,             \
+      int use_async_offload
+
+#define DGB_BWD_PARAMS(T)                                                                                       \
+  const T *eps_r_pad, const T *sigma_pad, const T *mu_r_pad, const void *E_saved, const void *R_saved,         \
+      T *lex, T *ley, T *lez, T *lhx, T *lhy, T *lhz, T *ce_hist, T *ce_curl, T *ce_rhs, T *ch_hist,           \
+      T *ch_curl, T *ch_rhs, T *x0e1, T *x0e2, T *x0h1, T *x0h2, T *xme1, T *xme2, T *xmh1, T *xmh2, T *y0e1,  \
+      T *y0e2, T *y0h1, T *y0h2, T *yme1, T *yme2, T *ymh1, T *ymh2, T *z0e1, T *z0e2, T *z0h1, T *z0h2,       \
+      T *zme1, T *zme2, T *zmh1, T *zmh2, int p0, int p1, int p2, int p3, int p4, int p5, const T *x0E,       \
+      const T *xmE, const T *y0E, const T *ymE, const T *z0E, const T *zmE, const T *x0H, const T *xmH,      \
+      const T *y0H, const T *ymH, const T *z0H, const T *zmH, T dt, int nt, int nshot, int nrx, T dx, T dy,   \
+      T dz, int NX, int NY, int NZ, int ndata, const int *rx_loc, const T *data_grad, int rx_comp, int nsrc,  \
+      const int *src_loc, int src_comp, T *grad_source, int want_src, T *grad_eps, T *grad_sig, int want_eps,  \
+      int want_sig, int S, int mode, int storage_type, int use_async_offload
+
+#define DGB_FILL_COMMON(cm)                                                                                     \
+  do {                                                                                                          \
+    (cm).g = make_grid(NX, NY, NZ, nshot);                                                                      \
+    (cm).dx = dx; (cm).dy = dy; (cm).dz = dz; (cm).dt = dt; (cm).nt = nt;                                       \
+    const int pp[6] = {p0, p1, p2, p3, p4, p5};                                                                 \
+    for (int f_ = 0; f_ < 6; ++f_) (cm).p[f_] = pp[f_];                                                         \
+    (cm).eps = eps_r_pad; (cm).sig = sigma_pad; (cm).mu = mu_r_pad;                                            \
+    (cm).ce_hist = ce_hist; (cm).ce_curl = ce_curl; (cm).ce_rhs = ce_rhs;                                      \
+    (cm).ch_hist = ch_hist; (cm).ch_curl = ch_curl; (cm).ch_rhs = ch_rhs;                                      \
+    (cm).eR[0] = x0E; (cm).eR[1] = xmE; (cm).eR[2] = y0E; (cm).eR[3] = ymE; (cm).eR[4] = z0E; (cm).eR[5] = zmE; \
+    (cm).hR[0] = x0H; (cm).hR[1] = xmH; (cm).hR[2] = y0H; (cm).hR[3] = ymH; (cm).hR[4] = z0H; (cm).hR[5] = zmH; \
+    (cm).S = S; (cm).mode = mode; (cm).storage_type = storage_type;                                            \
+  } while (0)
+
+template <typename T>
+static void forward_entry(ForwardCall<T>& fc) {
+  forward_impl<T>(fc);
+}
+
+#define DGB_FORWARD_BODY(T)                                                                                     \
+  ForwardCall<T> fc;                                                                                            \
+  memset(&fc, 0, sizeof(fc));                                                                                   \
+  DGB_FILL_COMMON(fc.cm);                                                                                       \
+  T* ep[12] = {x0e1, x0e2, xme1, xme2, y0e1, y0e2, yme1, yme2, z0e1, z0e2, zme1, zme2};                         \
+  T* hp[12] = {x0h1, x0h2, xmh1, xmh2, y0h1, y0h2, ymh1, ymh2, z0h1, z0h2, zmh1, zmh2};                         \
+  for (int q_ = 0; q_ < 12; ++q_) { fc.cm.ePsi[q_] = ep[q_]; fc.cm.hPsi[q_] = hp[q_]; }                         \
+  fc.E_saved = E_saved; fc.R_saved = R_saved;                                                                   \
+  fc.Ex = Ex; fc.Ey = Ey; fc.Ez = Ez; fc.Hx = Hx; fc.Hy = Hy; fc.Hz = Hz;                                       \
+  fc.nrx = nrx; fc.rx_loc = rx_loc; fc.rx = rx_out; fc.rx_comp = rx_comp;                                      \
+  fc.nsrc = nsrc; fc.src_loc = src_loc; fc.wave = src_wave; fc.src_comp = src_comp;                            \
+  fc.save_model_history = save_model_history;                                                                   \
+  (void)use_async_offload;                                                                                      \
+  forward_entry<T>(fc)
+
+#define DGB_BACKWARD_BODY(T)                                                                                    \
+  BackwardCall<T> bc;                                                                                           \
+  memset(&bc, 0, sizeof(bc));                                                                                   \
+  DGB_FILL_COMMON(bc.cm);                                                                                       \
+  T* ep[12] = {x0e1, x0e2, xme1, xme2, y0e1, y0e2, yme1, yme2, z0e1, z0e2, zme1, zme2};                         \
+  T* hp[12] = {x0h1, x0h2, xmh1, xmh2, y0h1, y0h2, ymh1, ymh2, z0h1, z0h2, zmh1, zmh2};                         \
+  for (int q_ = 0; q_ < 12; ++q_) { bc.cm.ePsi[q_] = ep[q_]; bc.cm.hPsi[q_] = hp[q_]; }                         \
+  bc.E_saved = E_saved; bc.R_saved = R_saved;                                                                   \
+  bc.lEx = lex; bc.lEy = ley; bc.lEz = lez; bc.lHx = lhx; bc.lHy = lhy; bc.lHz = lhz;                           \
+  bc.ndata = ndata; bc.rx_loc = rx_loc; bc.data_grad = data_grad; bc.rx_comp = rx_comp;                        \
+  bc.nsrc = nsrc; bc.src_loc = src_loc; bc.src_comp = src_comp;                                                 \
+  bc.grad_source = grad_source; bc.want_src = want_src;                                                         \
+  bc.grad_eps = grad_eps; bc.grad_sig = grad_sig; bc.want_eps = want_eps; bc.want_sig = want_sig;              \
+  (void)nrx; (void)use_async_offload;                                                                           \
+  backward_impl<T>(bc)
+
+DGB_API void forward(DGB_FWD_PARAMS(float)) { DGB_FORWARD_BODY(float); }
+DGB_API void backward(DGB_BWD_PARAMS(float)) { DGB_BACKWARD_BODY(float); }
+DGB_API void dgb_forward_f64(DGB_FWD_PARAMS(double)) { DGB_FORWARD_BODY(double); }
+DGB_API void dgb_backward_f64(DGB_BWD_PARAMS(double)) { DGB_BACKWARD_BODY(double); }
+
+DGB_API int deepgpr_abi_version(void) { return 6; }
+DGB_API int deepgpr_supports_error_reporting(void) { return 1; }
+DGB_API const char* deepgpr_last_error(void) { return g_error; }
+DGB_API void deepgpr_clear_last_error(void) { g_error[0] = '\0'; }
+DGB_API void deepgpr_clear_cuda_resource_cache(void) { g_error[0] = '\0'; }
+DGB_API int deepgpr_deterministic_adjoint(void) { return 1; }
+DGB_API int deepgpr_supports_external_pml(void) { return 1; }
+DGB_API int deepgpr_supports_pml_material_gradients(void) { return 1; }
+DGB_API int deepgpr_supports_int8_wavefield(void) { return 0; }
+DGB_API int deepgpr_supports_conversion_backends(void) { return 0; }
+DGB_API int deepgpr_supports_int8_reduction_backends(void) { return 0; }
+DGB_API int deepgpr_supports_rhs_reconstruction(void) { return 1; }
+DGB_API int deepgpr_supports_physical_history(void) { return 1; }
+DGB_API int deepgpr_supports_tm2d_fast_path(void) { return 1; }
+DGB_API void set_fdtd_order(int order) { g_order = (order == 4 || order == 8) ? order : 2; }
+
+DGB_API int dgb_version(void) { return 1; }
+DGB_API int dgb_supports_fp8_history(void) { return 1; }
+
+DGB_API int dgb_set_stream(void* stream) {
+  g_opt.user_stream = static_cast<cudaStream_t>(stream);
+  g_opt.user_stream_set = true;
+  return 0;
+}
+
+DGB_API void dgb_clear_stream(void) {
+  g_opt.user_stream = nullptr;
+  g_opt.user_stream_set = false;
+}
+
+DGB_API int dgb_set_options(int acc64, int chunk_steps, int use_graph, int fdtd_order) {
+  if (chunk_steps < 1 || chunk_steps > 4096) return -1;
+  g_opt.acc64 = acc64 ? 1 : 0;
+  g_opt.chunk = chunk_steps;
+  g_opt.use_graph = use_graph ? 1 : 0;
+  g_opt.order_override = (fdtd_order == 2 || fdtd_order == 4 || fdtd_order == 8) ? fdtd_order : 0;
+  return 0;
+}
+
+// Bytes of one history buffer (E_saved or R_saved) for a storage kind.
+DGB_API long long dgb_history_bytes(int kind, int ncomp, int nt_saved, int nshot, long long box_cells,
+                                    int NX, int NY, int NZ, int tm2d) {
+  const long long vals = (long long)ncomp * nt_saved * nshot * box_cells;
+  if (kind == kFP8) {
+    Grid g;
+    g.NX = NX; g.NY = NY; g.NZ = NZ;
+    const long long tiles = fp8_tiles(g, tm2d != 0);
+    return fp8_payload_bytes(vals) + (long long)ncomp * nt_saved * nshot * tiles * (long long)sizeof(float);
+  }
+  return vals * hist_elem_bytes(kind);
+}
