@@ -1,0 +1,368 @@
+#!/usr/bin/env python
+"""Benchmark: 2D multi-shot FWI gradient (forward + exact adjoint) on B200.
+
+Workload (one "step" = one full gradient evaluation): physical grid 400 x 800
+(dx = 0.01 m, CPML 10 -> 420 x 820 extended cells), 32 shots, 200 receivers
+per shot, nt = 3000, fdtd_order 4, gradient mode 2 (Ez), FP32 E-only history
+(132 GB, resident in HBM), Ricker 400 MHz, dt = 0.9 CFL, L2 misfit against
+data of the same model with an eps_r = 9 disc.  Models are seeded synthetic
+(deepgpr_b200.synthetic.fwi_2d); no dataset is read.
+
+metric: cell-updates/s = 2 (forward + adjoint) x extended cells x nt x shots
+per step / device time.  Inputs (fields 132 MB, history 132 GB) are larger
+than L2, so no flush is needed between steps.
+
+Multi-GPU (torchrun): every rank solves its own 32 shots (weak scaling) and
+the material gradient is summed with one NCCL all-reduce per step.
+
+``--impl reference`` times the reference's own C/OpenMP CPU backend
+(oracle/_ref, compiled from the reference source) on a bounded sample of the
+same workload with all host threads.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+import torch  # noqa: E402
+
+METRIC = "cell-updates/s"
+UNIT = "cell-updates/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
+    ap.add_argument("--nt", type=int, default=3000)
+    ap.add_argument("--shots", type=int, default=32)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def dist_setup(n: int):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(local)
+    return rank, world, local
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = Path("/tmp") / f"bench_clocks_{os.getpid()}.csv"
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None or not self.path.is_file():
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, mx, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in self.path.read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        self.path.unlink(missing_ok=True)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        busy = [v for v in sm if v > 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(busy), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.is_file():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# Algorithmic bytes per shot-cell per launch of each 2D TM kernel (FP32):
+# every array a kernel must read or write once, coefficients per shot
+# (one shot per CTA), E^n history write in the H kernel (E-only history).
+BYTES_PER_CELL_2D = {
+    "fwd_h": 4 + 8 + 8 + 4 + 4,      # Ez r, Hx rw, Hy rw, ch_curl r, E^n w
+    "fwd_e": 4 + 4 + 8 + 4 + 4,      # Hy r, Hx r, Ez rw, ce_hist r, ce_curl r
+    "adj_e": 4 + 4 + 8 + 8,          # lEz r, ce_curl r, lHx rw, lHy rw
+    "adj_h": 4 + 4 + 4 + 8 + 4,      # lHy r, ch_curl r, lHx r, lEz rw, ce_hist r
+    "image": 4 + 4 + 4,              # lEz, E^n, E^(n+1) per shot (per-cell terms amortised)
+}
+
+
+def ours(args, rank, world, local):
+    import deepgpr_b200 as dg
+    from deepgpr_b200 import native
+    from deepgpr_b200.synthetic import fwi_2d
+
+    dev = torch.device("cuda", local)
+    acq = fwi_2d(seed=1002 + rank, nt=args.nt, nshot=args.shots)
+    nx, ny = acq.eps_r.shape
+    ext_cells = (nx + 20) * (ny + 20)
+    shots = acq.sources.shape[0]
+    units_per_step = 2 * ext_cells * args.nt * shots
+
+    common = dict(dx=acq.dx, dt=acq.dt, pmlthick=10, fdtd_order=acq.order, mode=2)
+    src_d, rcv_d = acq.sources.to(dev), acq.receivers.to(dev)
+    wave_d = acq.wavelet.to(dev)
+    with torch.no_grad():
+        obs = dg.compute(dev, source_amplitudes=wave_d, source_location=src_d, receiver_location=rcv_d,
+                         eps_r=acq.eps_true.to(dev), sigma=acq.sigma.to(dev), save_wavefield_history=False,
+                         **common)[-1].clone()
+    eps0, sig0 = acq.eps_r.to(dev), acq.sigma.to(dev)
+
+    def gradient(eps_in, sig_in, wave, src, rcv, data):
+        eps = eps_in.detach().requires_grad_(True)
+        sig = sig_in.detach().requires_grad_(True)
+        out = dg.compute(dev, source_amplitudes=wave, source_location=src, receiver_location=rcv, eps_r=eps,
+                         sigma=sig, **common)
+        loss = 0.5 * ((out[-1] - data) ** 2).sum()
+        del out
+        loss.backward()
+        ge, gs = eps.grad, sig.grad
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.all_reduce(ge)
+            dist.all_reduce(gs)
+        return loss.detach(), ge, gs
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        gradient(eps0, sig0, wave_d, src_d, rcv_d, obs)
+    barrier()
+    launches0 = native.launch_count()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clocks:
+        start.record()
+        for _ in range(args.steps):
+            loss, ge, gs = gradient(eps0, sig0, wave_d, src_d, rcv_d, obs)
+        stop.record()
+        barrier()
+    launches = native.launch_count() - launches0
+    ms = start.elapsed_time(stop)
+    ms_max = ms
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    value = units_per_step * world * args.steps / (ms_max / 1e3)
+
+    # end to end: host (pinned) inputs copied in and the loss + gradients copied out every step
+    e2e = None
+    if not args.no_e2e:
+        h_eps, h_sig = acq.eps_r.pin_memory(), acq.sigma.pin_memory()
+        h_wave, h_src, h_rcv = acq.wavelet.pin_memory(), acq.sources.pin_memory(), acq.receivers.pin_memory()
+        h_obs = obs.cpu().pin_memory()
+        out_loss = torch.empty((), pin_memory=True)
+        out_ge = torch.empty_like(h_eps).pin_memory()
+        out_gs = torch.empty_like(h_sig).pin_memory()
+        h2d = sum(t.numel() * t.element_size() for t in (h_eps, h_sig, h_wave, h_src, h_rcv, h_obs))
+        d2h = sum(t.numel() * t.element_size() for t in (out_loss, out_ge, out_gs))
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            d_eps = h_eps.to(dev, non_blocking=True)
+            d_sig = h_sig.to(dev, non_blocking=True)
+            d_wave = h_wave.to(dev, non_blocking=True)
+            d_src = h_src.to(dev, non_blocking=True)
+            d_rcv = h_rcv.to(dev, non_blocking=True)
+            d_obs = h_obs.to(dev, non_blocking=True)
+            loss, ge, gs = gradient(d_eps, d_sig, d_wave, d_src, d_rcv, d_obs)
+            out_loss.copy_(loss, non_blocking=True)
+            out_ge.copy_(ge, non_blocking=True)
+            out_gs.copy_(gs, non_blocking=True)
+        e1.record()
+        barrier()
+        ems = e0.elapsed_time(e1)
+        if world > 1:
+            import torch.distributed as dist
+
+            t = torch.tensor([ems], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        e2e = {"value": units_per_step * world * args.steps / (ems / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "ms_per_step": ems / args.steps}
+
+    # roofline of the dominant kernel: CUDA-event time of every launch in one profiled step
+    native.profile(True)
+    gradient(eps0, sig0, wave_d, src_d, rcv_d, obs)
+    torch.cuda.synchronize()
+    prof = native.profile_read()
+    native.profile(False)
+    peak, peak_kind = peaks()
+    dom = max(prof, key=lambda k: prof[k][0])
+    dom_ms, dom_n = prof[dom]
+    shot_cells = (nx + 21) * (ny + 21) * shots   # field grid incl. halo, all shots of this rank
+    alg = BYTES_PER_CELL_2D[dom] * shot_cells
+    achieved = alg / (dom_ms / max(dom_n, 1) / 1e3) / 1e9
+    traffic = None
+    tf = ROOT / "profiles" / "ncu_traffic.json"
+    if tf.is_file():
+        per_cell = json.loads(tf.read_text()).get("bytes_per_shot_cell", {}).get(dom)
+        if per_cell is not None:
+            traffic = float(per_cell) * shot_cells
+    total_prof = sum(v[0] for v in prof.values())
+    roofline = {
+        "bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+        "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_kind,
+        "algorithmic_bytes_per_launch": alg,
+        "kernel_share": {k: round(v[0] / total_prof, 4) for k, v in prof.items() if v[1]},
+        "avg_launch_us": {k: round(v[0] / v[1] * 1e3, 2) for k, v in prof.items() if v[1]},
+    }
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(args.shots, budget_s=15.0)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded layered model + random field)",
+            "config": {"workload": "2D multi-shot FWI gradient (forward + adjoint)", "grid": [nx, ny, 1],
+                       "extended": [nx + 20, ny + 20, 1], "shots_per_gpu": shots, "receivers": 200, "nt": args.nt,
+                       "fdtd_order": 4, "mode": 2, "history": "FP32 E-only (resident)",
+                       "l2_policy": "inputs larger than L2 (132 MB fields, 132 GB history)"},
+            "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "clocks": clocks.summary(), "loss": float(loss),
+        }
+        print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(shots: int, budget_s: float = 15.0, steps_hint: int = 0):
+    """Reference C/OpenMP backend (oracle/_ref) on a bounded sample: nt truncated."""
+    from oracle import driver
+
+    from deepgpr_b200.synthetic import fwi_2d
+
+    kind = "reference" if driver.available("ref") else "port"
+    lib = "ref" if kind == "reference" else "oracle"
+    cores = os.cpu_count() or 1
+
+    def run(nt):
+        acq = fwi_2d(seed=1002, nt=nt, nshot=shots)
+        p = driver.Problem(eps_r=acq.eps_r, sigma=acq.sigma, source_amplitudes=acq.wavelet,
+                           source_location=acq.sources, receiver_location=acq.receivers, dx=acq.dx, dt=acq.dt,
+                           pml=10, order=4, mode=2)
+        out = driver.run(p, lib)
+        return out["t_forward"] + out["t_backward"], acq
+
+    t, acq = run(2)
+    nt = max(2, min(200, int(2 * budget_s / max(t, 1e-3))))
+    t, acq = run(nt)
+    nx, ny = acq.eps_r.shape
+    units = 2 * (nx + 20) * (ny + 20) * nt * shots
+    return {"value": units / t, "unit": UNIT, "cores": cores, "kind": kind,
+            "sample": f"same workload with nt truncated to {nt} steps, {shots} shots; native forward + "
+                      f"backward time {t:.1f} s (host preprocessing excluded)"}
+
+
+def reference(args, rank, world):
+    if rank != 0:
+        return
+    samples = []
+    cpu = None
+    for i in range(args.warmup + args.steps):
+        c = cpu_baseline(args.shots, budget_s=8.0)
+        if i >= args.warmup:
+            samples.append(c["value"])
+            cpu = c
+    value = statistics.median(samples)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded layered model + random field)", "impl": "reference",
+        "config": {"workload": "2D multi-shot FWI gradient (forward + adjoint)", "grid": [400, 800, 1],
+                   "shots": args.shots, "nt": args.nt, "fdtd_order": 4, "mode": 2,
+                   "sample": "nt truncated per step (CPU)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cpu["cores"], "kind": cpu["kind"],
+                         "sample": cpu["sample"]},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_setup(args.gpus)
+    try:
+        if args.impl == "reference":
+            reference(args, rank, world)
+        else:
+            ours(args, rank, world, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -48,6 +48,50 @@ struct ThreadOptions {
 };
 thread_local ThreadOptions g_opt;
 
+// Kernel timing (dgb_profile): when enabled, time steps are launched without
+// graph capture and every grid kernel is bracketed by CUDA events on the
+// library stream; durations are summed per kernel kind.
+enum KernelKind { KK_FWD_H = 0, KK_FWD_E, KK_ADJ_E, KK_ADJ_H, KK_IMAGE, KK_COUNT };
+struct ProfileState {
+  bool on = false;
+  double ms[KK_COUNT] = {0};
+  long long launches[KK_COUNT] = {0};
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
+};
+thread_local ProfileState g_prof;
+thread_local long long g_launch_count = 0;   // grid kernels launched by this thread
+
+// Launch `fn` (which enqueues one kernel on st), timing it when profiling.
+template <typename F>
+void timed(int kind, cudaStream_t st, F fn) {
+  ++g_launch_count;
+  if (!g_prof.on) {
+    fn();
+    return;
+  }
+  cudaEvent_t a = nullptr, b = nullptr;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  cudaEventRecord(a, st);
+  fn();
+  cudaEventRecord(b, st);
+  g_prof.pending.push_back({kind, {a, b}});
+}
+
+void harvest_profile() {
+  for (auto& p : g_prof.pending) {
+    cudaEventSynchronize(p.second.second);
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, p.second.first, p.second.second) == cudaSuccess) {
+      g_prof.ms[p.first] += ms;
+      g_prof.launches[p.first] += 1;
+    }
+    cudaEventDestroy(p.second.first);
+    cudaEventDestroy(p.second.second);
+  }
+  g_prof.pending.clear();
+}
+
 void set_error(const char* fmt, ...) {
   va_list ap;
   va_start(ap, fmt);
@@ -326,17 +370,21 @@ template <typename Issue>
 bool run_loop(int steps, int dir, Control* ctrl, cudaStream_t st, Issue issue) {
   const int chunk = std::max(1, g_opt.chunk);
   cudaGraphExec_t exec = nullptr;
+  long long per_replay = 0;
   bool ok = true;
   int t = 0;
   while (ok && t < steps) {
     const int K = std::min(chunk, steps - t);
-    if (g_opt.use_graph && K == chunk && steps >= 2 * chunk) {
+    if (g_opt.use_graph && !g_prof.on && K == chunk && steps >= 2 * chunk) {
       if (!exec) {
         cudaGraph_t graph = nullptr;
         ok = cuda_ok(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
         if (!ok) break;
+        const long long before = g_launch_count;
         for (int k = 0; k < K; ++k) issue(k);
         k_advance<<<1, 1, 0, st>>>(ctrl, dir * K);
+        per_replay = g_launch_count - before + 1;
+        g_launch_count = before;
         cudaError_t e1 = cudaGetLastError();
         cudaError_t e2 = cudaStreamEndCapture(st, &graph);
         ok = cuda_ok(e1, "capture launch") && cuda_ok(e2, "end capture");
@@ -346,10 +394,13 @@ bool run_loop(int steps, int dir, Control* ctrl, cudaStream_t st, Issue issue) {
         if (!ok) break;
       }
       ok = cuda_ok(cudaGraphLaunch(exec, st), "graph launch");
+      g_launch_count += per_replay;
     } else {
       for (int k = 0; k < K; ++k) issue(k);
       k_advance<<<1, 1, 0, st>>>(ctrl, dir * K);
+      ++g_launch_count;
       ok = cuda_ok(cudaGetLastError(), "time-step launch");
+      if (g_prof.on) harvest_profile();
     }
     t += K;
   }
@@ -522,13 +573,27 @@ void forward_impl(const ForwardCall<T>& fc) {
         TiledFwd<T> b = P;
         b.a.k_in_chunk = k;
         if (tm2d) {
-          if (R == 1) { k2_fwd_h<T, 1><<<grid, T2, 0, st>>>(b, tf); k2_fwd_e<T, 1><<<grid, T2, 0, st>>>(b, tf); }
-          else if (R == 2) { k2_fwd_h<T, 2><<<grid, T2, 0, st>>>(b, tf); k2_fwd_e<T, 2><<<grid, T2, 0, st>>>(b, tf); }
-          else { k2_fwd_h<T, 4><<<grid, T2, 0, st>>>(b, tf); k2_fwd_e<T, 4><<<grid, T2, 0, st>>>(b, tf); }
+          timed(KK_FWD_H, st, [&] {
+            if (R == 1) k2_fwd_h<T, 1><<<grid, T2, 0, st>>>(b, tf);
+            else if (R == 2) k2_fwd_h<T, 2><<<grid, T2, 0, st>>>(b, tf);
+            else k2_fwd_h<T, 4><<<grid, T2, 0, st>>>(b, tf);
+          });
+          timed(KK_FWD_E, st, [&] {
+            if (R == 1) k2_fwd_e<T, 1><<<grid, T2, 0, st>>>(b, tf);
+            else if (R == 2) k2_fwd_e<T, 2><<<grid, T2, 0, st>>>(b, tf);
+            else k2_fwd_e<T, 4><<<grid, T2, 0, st>>>(b, tf);
+          });
         } else {
-          if (R == 1) { k3_fwd_h<T, 1><<<grid, 256, 0, st>>>(b); k3_fwd_e<T, 1><<<grid, 256, 0, st>>>(b); }
-          else if (R == 2) { k3_fwd_h<T, 2><<<grid, 256, 0, st>>>(b); k3_fwd_e<T, 2><<<grid, 256, 0, st>>>(b); }
-          else { k3_fwd_h<T, 4><<<grid, 256, 0, st>>>(b); k3_fwd_e<T, 4><<<grid, 256, 0, st>>>(b); }
+          timed(KK_FWD_H, st, [&] {
+            if (R == 1) k3_fwd_h<T, 1><<<grid, 256, 0, st>>>(b);
+            else if (R == 2) k3_fwd_h<T, 2><<<grid, 256, 0, st>>>(b);
+            else k3_fwd_h<T, 4><<<grid, 256, 0, st>>>(b);
+          });
+          timed(KK_FWD_E, st, [&] {
+            if (R == 1) k3_fwd_e<T, 1><<<grid, 256, 0, st>>>(b);
+            else if (R == 2) k3_fwd_e<T, 2><<<grid, 256, 0, st>>>(b);
+            else k3_fwd_e<T, 4><<<grid, 256, 0, st>>>(b);
+          });
         }
       };
       ok = run_loop(cm.nt, +1, ctrl, st, issue);
@@ -808,15 +873,30 @@ void backward_impl(const BackwardCall<T>& bc) {
       auto issue = [&](int k) {
         TiledAdj<T> b = P;
         b.a.k_in_chunk = k;
-        if (want_model && img_blocks > 0) k_image<T><<<img_blocks, 256, 0, st>>>(b.a, lamx, lamy, lamz, tm2d ? 1 : 0);
+        if (want_model && img_blocks > 0)
+          timed(KK_IMAGE, st, [&] { k_image<T><<<img_blocks, 256, 0, st>>>(b.a, lamx, lamy, lamz, tm2d ? 1 : 0); });
         if (tm2d) {
-          if (R == 1) { k2_adj_e<T, 1><<<grid, T2, 0, st>>>(b, tl); k2_adj_h<T, 1, false><<<grid, T2, 0, st>>>(b, tl); }
-          else if (R == 2) { k2_adj_e<T, 2><<<grid, T2, 0, st>>>(b, tl); k2_adj_h<T, 2, false><<<grid, T2, 0, st>>>(b, tl); }
-          else { k2_adj_e<T, 4><<<grid, T2, 0, st>>>(b, tl); k2_adj_h<T, 4, false><<<grid, T2, 0, st>>>(b, tl); }
+          timed(KK_ADJ_E, st, [&] {
+            if (R == 1) k2_adj_e<T, 1><<<grid, T2, 0, st>>>(b, tl);
+            else if (R == 2) k2_adj_e<T, 2><<<grid, T2, 0, st>>>(b, tl);
+            else k2_adj_e<T, 4><<<grid, T2, 0, st>>>(b, tl);
+          });
+          timed(KK_ADJ_H, st, [&] {
+            if (R == 1) k2_adj_h<T, 1, false><<<grid, T2, 0, st>>>(b, tl);
+            else if (R == 2) k2_adj_h<T, 2, false><<<grid, T2, 0, st>>>(b, tl);
+            else k2_adj_h<T, 4, false><<<grid, T2, 0, st>>>(b, tl);
+          });
         } else {
-          if (R == 1) { k3_adj_e<T, 1><<<grid, 256, 0, st>>>(b); k3_adj_h<T, 1, false><<<grid, 256, 0, st>>>(b); }
-          else if (R == 2) { k3_adj_e<T, 2><<<grid, 256, 0, st>>>(b); k3_adj_h<T, 2, false><<<grid, 256, 0, st>>>(b); }
-          else { k3_adj_e<T, 4><<<grid, 256, 0, st>>>(b); k3_adj_h<T, 4, false><<<grid, 256, 0, st>>>(b); }
+          timed(KK_ADJ_E, st, [&] {
+            if (R == 1) k3_adj_e<T, 1><<<grid, 256, 0, st>>>(b);
+            else if (R == 2) k3_adj_e<T, 2><<<grid, 256, 0, st>>>(b);
+            else k3_adj_e<T, 4><<<grid, 256, 0, st>>>(b);
+          });
+          timed(KK_ADJ_H, st, [&] {
+            if (R == 1) k3_adj_h<T, 1, false><<<grid, 256, 0, st>>>(b);
+            else if (R == 2) k3_adj_h<T, 2, false><<<grid, 256, 0, st>>>(b);
+            else k3_adj_h<T, 4, false><<<grid, 256, 0, st>>>(b);
+          });
         }
       };
       if (ok) ok = run_loop(cm.nt, -1, ctrl, st, issue);
@@ -962,6 +1042,30 @@ DGB_API int deepgpr_supports_tm2d_fast_path(void) { return 1; }
 DGB_API void set_fdtd_order(int order) { g_order = (order == 4 || order == 8) ? order : 2; }
 
 DGB_API int dgb_version(void) { return 1; }
+
+// Kernel timing of the calling thread: enable/disable (clears the totals on
+// enable) and read the per-kind totals (fwd_h, fwd_e, adj_e, adj_h, image).
+DGB_API void dgb_profile(int enable) {
+  g_prof.on = enable != 0;
+  if (g_prof.on)
+    for (int k = 0; k < KK_COUNT; ++k) {
+      g_prof.ms[k] = 0.0;
+      g_prof.launches[k] = 0;
+    }
+}
+
+// Number of kernels this thread has launched through the library so far
+// (graph replays count every kernel node).
+DGB_API long long dgb_launch_count(void) { return g_launch_count; }
+
+DGB_API int dgb_profile_read(double* ms, long long* launches, int n) {
+  const int m = n < KK_COUNT ? n : KK_COUNT;
+  for (int k = 0; k < m; ++k) {
+    ms[k] = g_prof.ms[k];
+    launches[k] = g_prof.launches[k];
+  }
+  return KK_COUNT;
+}
 DGB_API int dgb_supports_fp8_history(void) { return 1; }
 
 DGB_API int dgb_set_stream(void* stream) {

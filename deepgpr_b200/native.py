@@ -102,7 +102,32 @@ SCALAR_SYMBOLS: Dict[str, Tuple[Tuple[str, ...], Optional[str]]] = {
     "dgb_clear_stream": ((), None),
     "dgb_set_options": (("int", "int", "int", "int"), "int"),
     "dgb_history_bytes": (("int", "int", "int", "int", "long long", "int", "int", "int", "int"), "long long"),
+    "dgb_profile": (("int",), None),
+    "dgb_launch_count": ((), "long long"),
+    "dgb_profile_read": (("void*", "void*", "int"), "int"),
 }
+
+KERNEL_KINDS = ("fwd_h", "fwd_e", "adj_e", "adj_h", "image")
+
+
+def profile(enable: bool) -> None:
+    """Enable per-kernel CUDA-event timing for this thread (no graph replay while on)."""
+    load_library().dgb_profile(int(enable))
+
+
+def launch_count() -> int:
+    """Kernels launched by this thread through the library (time-step kernels)."""
+    return int(load_library().dgb_launch_count())
+
+
+def profile_read() -> Dict[str, Tuple[float, int]]:
+    """Per-kernel-kind (total ms, launches) since ``profile(True)``."""
+    lib = load_library()
+    n = len(KERNEL_KINDS)
+    ms = (ctypes.c_double * n)()
+    cnt = (ctypes.c_longlong * n)()
+    lib.dgb_profile_read(ctypes.cast(ms, ctypes.c_void_p), ctypes.cast(cnt, ctypes.c_void_p), n)
+    return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(KERNEL_KINDS)}
 
 SOLVER_SYMBOLS = {
     "forward": (FORWARD_SIGNATURE, "float"),

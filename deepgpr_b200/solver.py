@@ -380,8 +380,6 @@ def compute(
     device = torch.device(device)
     if device.type != "cuda":
         raise NativeLibraryError("deepgpr_b200 solves on CUDA devices only (there is no CPU backend).")
-    if device.index is None:
-        device = torch.device("cuda", torch.cuda.current_device())
     if fdtd_order not in SUPPORTED_FDTD_ORDERS:
         raise ValueError("fdtd_order must be one of 2, 4, or 8.")
     if mode not in SUPPORTED_GRADIENT_MODES:
@@ -421,6 +419,8 @@ def compute(
     if getattr(mu_r, "requires_grad", False):
         raise NotImplementedError("Relative-permeability gradients are not provided.")
 
+    if device.index is None:
+        device = torch.device("cuda", torch.cuda.current_device())
     spacing = normalize_grid_spacing(dx)
     prepared = prepare_model(device, eps_r, sigma, mu_r, source_amplitudes, source_location, receiver_location,
                              spacing, dt, pmlthick, fdtd_order, dtype=precision)

@@ -15,6 +15,7 @@ from __future__ import annotations
 
 import ctypes
 import subprocess
+import time
 from dataclasses import dataclass, field
 from pathlib import Path
 from typing import Any, Dict, Optional, Sequence, Tuple
@@ -165,12 +166,16 @@ def run(p: Problem, kind: str = "oracle", backward: bool = True) -> Dict[str, An
     args = forward_arguments(cfg, tensors, states, e_saved, r_saved, rx, waveform, stype, want_model)
     lib.deepgpr_clear_last_error()
     lib.set_fdtd_order(p.order)
-    lib.forward(*native.marshal(native.FORWARD_SIGNATURE, args))
+    fargs = native.marshal(native.FORWARD_SIGNATURE, args)
+    t0 = time.perf_counter()
+    lib.forward(*fargs)
+    t_forward = time.perf_counter() - t0
     err = lib.deepgpr_last_error()
     if err:
         raise RuntimeError(f"{kind} forward: {err.decode()}")
     out: Dict[str, Any] = {"receivers": rx.clone(), "states": [s.clone() for s in states],
-                           "E_saved": e_saved.clone(), "R_saved": r_saved.clone(), "storage_type": stype}
+                           "E_saved": e_saved.clone(), "R_saved": r_saved.clone(), "storage_type": stype,
+                           "t_forward": t_forward}
     if not backward:
         return out
     data_grad = (2.0 * rx) if p.data_grad is None else p.data_grad.float().contiguous().clone()
@@ -184,7 +189,10 @@ def run(p: Problem, kind: str = "oracle", backward: bool = True) -> Dict[str, An
                               (p.want_source, p.want_eps, p.want_sigma), stype)
     lib.deepgpr_clear_last_error()
     lib.set_fdtd_order(p.order)
-    lib.backward(*native.marshal(native.BACKWARD_SIGNATURE, args))
+    bargs = native.marshal(native.BACKWARD_SIGNATURE, args)
+    t0 = time.perf_counter()
+    lib.backward(*bargs)
+    out["t_backward"] = time.perf_counter() - t0
     err = lib.deepgpr_last_error()
     if err:
         raise RuntimeError(f"{kind} backward: {err.decode()}")

@@ -1,0 +1,137 @@
+"""Host-side logic of the product package (no GPU): options, validation, layouts."""
+
+from __future__ import annotations
+
+import pytest
+import torch
+
+import deepgpr_b200 as dg
+from deepgpr_b200 import config
+from deepgpr_b200.errors import CFLConditionError, NativeLibraryError
+from deepgpr_b200.model import prepare_model, shift_locations
+from deepgpr_b200.solver import _tm2d_applies
+from deepgpr_b200.storage import (
+    StorageConfig,
+    decode_fp8_history,
+    encode_storage_type,
+    fp8_tiles,
+    history_box,
+    resolve_rhs_reconstruction,
+    saved_history_shape,
+)
+
+
+def _inputs(nt=10, shape=(20, 16)):
+    eps = torch.full(shape, 4.0)
+    sig = torch.zeros(shape)
+    src = torch.tensor([[[5, 5, 0]]], dtype=torch.int32)
+    rcv = torch.tensor([[[6, 6, 0]]], dtype=torch.int32)
+    return eps, sig, torch.ones(1, nt), src, rcv
+
+
+def test_storage_word_matches_reference_bits():
+    cfg = StorageConfig(torch.float32, "none", config.STORAGE_FLOAT32)
+    assert encode_storage_type(cfg, True) == 0
+    assert encode_storage_type(cfg, False) == 1 << 26
+    assert encode_storage_type(cfg, True, rhs_from_e=True) == 1 << 4
+    assert encode_storage_type(cfg, True, physical=True) == 1 << 5
+    assert encode_storage_type(cfg, True, tm2d=True) == 1 << 6
+    bf = StorageConfig(torch.bfloat16, "none", config.STORAGE_BFLOAT16)
+    assert encode_storage_type(bf, True) == 2
+    fp8 = StorageConfig(torch.uint8, "fp8", config.STORAGE_FP8_E4M3)
+    assert encode_storage_type(fp8, True) & 0xF == 4
+
+
+def test_history_shapes_and_boxes():
+    assert saved_history_shape(2, 5, 3, 10, 11, 1) == (5, 3, 10, 11, 1)
+    assert saved_history_shape(3, 5, 3, 10, 11, 12) == (3, 5, 3, 10, 11, 12)
+    assert history_box(40, 30, 1, [10, 10, 5, 5, 0, 0], "physical") == ((10, 5, 0), (20, 20, 1))
+    assert history_box(40, 30, 1, [10, 10, 5, 5, 0, 0], "extended") == ((0, 0, 0), (40, 30, 1))
+
+
+def test_rhs_reconstruction_rules():
+    assert resolve_rhs_reconstruction("auto", 1, True, True) is True
+    assert resolve_rhs_reconstruction("auto", 2, True, True) is False
+    assert resolve_rhs_reconstruction("auto", 1, True, False) is False
+    assert resolve_rhs_reconstruction("stored", 1, True, True) is False
+    with pytest.raises(ValueError):
+        resolve_rhs_reconstruction("reconstructed", 3, True, True)
+
+
+def test_fp8_decoder_roundtrip():
+    torch.manual_seed(0)
+    field_shape = (9, 140, 2)
+    hx, hy, hz = 8, 139, 1
+    vals = torch.randn(2, 3, hx, hy, hz)
+    tiles = fp8_tiles(field_shape, True)
+    nvals = vals.numel()
+    payload = (nvals + 255) // 256 * 256
+    packed = torch.zeros(payload + 2 * 3 * tiles * 4, dtype=torch.uint8)
+    scales = torch.full((2, 3, tiles), 0.01)
+    q = (vals / 0.01).clamp(-448, 448).to(torch.float8_e4m3fn)
+    packed[:nvals] = q.reshape(-1).view(torch.uint8)
+    packed[payload:] = scales.reshape(-1).view(torch.uint8)
+    out = decode_fp8_history(packed, (2, 3, hx, hy, hz), field_shape, (0, 0, 0), tm2d=True)
+    assert torch.allclose(out, q.float() * 0.01)
+
+
+def test_tm2d_decision():
+    zeros = [torch.zeros(1)] * 30
+    assert _tm2d_applies(2, 2, 2, True, zeros, False)
+    assert not _tm2d_applies(3, 2, 2, True, zeros, False)
+    assert not _tm2d_applies(2, 0, 2, True, zeros, False)
+    assert not _tm2d_applies(2, 2, 3, True, zeros, False)
+    assert _tm2d_applies(2, 2, 3, False, zeros, False)
+    states = [torch.zeros(2) for _ in range(30)]
+    states[0] = torch.ones(2)   # nonzero Ex
+    assert not _tm2d_applies(2, 2, 2, True, states, True)
+
+
+def test_prepare_model_extends_and_validates():
+    eps, sig, w, src, rcv = _inputs()
+    p = prepare_model("cpu", eps, sig, None, w, src, rcv, 0.02, 1e-11, 3, 4)
+    assert (p.nx, p.ny, p.nz) == (26, 22, 1)
+    assert p.eps_r_pad.shape == (27, 23, 2)
+    assert p.pml == (3, 3, 3, 3, 0, 0)
+    assert shift_locations(src, p.pml, "cpu").tolist() == [[[8, 8, 0]]]
+    with pytest.raises(ValueError):
+        prepare_model("cpu", eps * 0.1, sig, None, w, src, rcv, 0.02, 1e-11, 3, 4)
+    with pytest.raises(ValueError):
+        prepare_model("cpu", eps, sig, None, w, src + 100, rcv, 0.02, 1e-11, 3, 4)
+    with pytest.raises(CFLConditionError):
+        prepare_model("cpu", eps, sig, None, w, src, rcv, 0.02, 1e-9, 3, 4)
+    with pytest.raises(ValueError):
+        prepare_model("cpu", eps, sig, None, w, src, rcv, 0.02, 1e-11, [1, 1, 1, 1, 1, 1], 4)
+
+
+def test_compute_requires_cuda():
+    eps, sig, w, src, rcv = _inputs()
+    with pytest.raises(NativeLibraryError):
+        dg.compute("cpu", dx=0.02, dt=1e-11, source_amplitudes=w, source_location=src, receiver_location=rcv,
+                   eps_r=eps, sigma=sig)
+
+
+def test_compute_option_errors_match_reference():
+    eps, sig, w, src, rcv = _inputs()
+    with pytest.raises(ValueError):
+        dg.compute("cuda", dx=0.02, dt=1e-11, source_amplitudes=w, source_location=src, receiver_location=rcv,
+                   eps_r=eps, sigma=sig, fdtd_order=6)
+    with pytest.raises(ValueError):
+        dg.compute("cuda", dx=0.02, dt=1e-11, source_amplitudes=w, source_location=src, receiver_location=rcv,
+                   eps_r=eps, sigma=sig, mode=4)
+    with pytest.raises(NotImplementedError):
+        dg.compute("cuda", dx=0.02, dt=1e-11, source_amplitudes=w, source_location=src, receiver_location=rcv,
+                   eps_r=eps, sigma=sig, wavefield_compression="int8")
+    with pytest.raises(ValueError):
+        dg.compute("cuda", dx=0.02, dt=1e-11, source_amplitudes=w, source_location=src, receiver_location=rcv,
+                   eps_r=eps, sigma=sig, save_wavefield_history=False, use_async_offload=True)
+
+
+def test_checkpoint_initial_field_shapes():
+    eps, sig, w, src, rcv = _inputs()
+    E, H, P = dg.checkpoint_initial_field("cpu", dx=0.02, dt=1e-11, source_amplitudes=w, source_location=src,
+                                          receiver_location=rcv, er=eps, se=sig, pmlthick=2)
+    assert all(t.shape == (1, 25, 21, 2) for t in (*E, *H))
+    assert len(P) == 24
+    assert P[0].shape == (1, 3, 20, 2)      # x0 E psi1: (nstep, p+1, ny, nz+1)
+    assert P[16].numel() == 0               # z faces disabled in 2D
