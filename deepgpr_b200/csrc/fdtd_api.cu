@@ -16,6 +16,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <atomic>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -52,14 +53,16 @@ thread_local ThreadOptions g_opt;
 // graph capture and every grid kernel is bracketed by CUDA events on the
 // library stream; durations are summed per kernel kind.
 enum KernelKind { KK_FWD_H = 0, KK_FWD_E, KK_ADJ_E, KK_ADJ_H, KK_IMAGE, KK_COUNT };
+// Process-wide (the autograd engine runs backward on its own thread).
 struct ProfileState {
-  bool on = false;
+  std::atomic<bool> on{false};
+  std::mutex mu;
   double ms[KK_COUNT] = {0};
   long long launches[KK_COUNT] = {0};
-  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
 };
-thread_local ProfileState g_prof;
-thread_local long long g_launch_count = 0;   // grid kernels launched by this thread
+ProfileState g_prof;
+thread_local std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> g_pending;
+std::atomic<long long> g_launch_count{0};   // time-step kernels launched by the library
 
 // Launch `fn` (which enqueues one kernel on st), timing it when profiling.
 template <typename F>
@@ -75,21 +78,22 @@ void timed(int kind, cudaStream_t st, F fn) {
   cudaEventRecord(a, st);
   fn();
   cudaEventRecord(b, st);
-  g_prof.pending.push_back({kind, {a, b}});
+  g_pending.push_back({kind, {a, b}});
 }
 
 void harvest_profile() {
-  for (auto& p : g_prof.pending) {
+  for (auto& p : g_pending) {
     cudaEventSynchronize(p.second.second);
     float ms = 0.0f;
     if (cudaEventElapsedTime(&ms, p.second.first, p.second.second) == cudaSuccess) {
+      std::lock_guard<std::mutex> lock(g_prof.mu);
       g_prof.ms[p.first] += ms;
       g_prof.launches[p.first] += 1;
     }
     cudaEventDestroy(p.second.first);
     cudaEventDestroy(p.second.second);
   }
-  g_prof.pending.clear();
+  g_pending.clear();
 }
 
 void set_error(const char* fmt, ...) {
@@ -380,11 +384,11 @@ bool run_loop(int steps, int dir, Control* ctrl, cudaStream_t st, Issue issue) {
         cudaGraph_t graph = nullptr;
         ok = cuda_ok(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
         if (!ok) break;
-        const long long before = g_launch_count;
+        const long long before = g_launch_count.load();
         for (int k = 0; k < K; ++k) issue(k);
         k_advance<<<1, 1, 0, st>>>(ctrl, dir * K);
-        per_replay = g_launch_count - before + 1;
-        g_launch_count = before;
+        per_replay = g_launch_count.load() - before + 1;
+        g_launch_count -= per_replay - 1;   // captured, not yet launched
         cudaError_t e1 = cudaGetLastError();
         cudaError_t e2 = cudaStreamEndCapture(st, &graph);
         ok = cuda_ok(e1, "capture launch") && cuda_ok(e2, "end capture");
@@ -1046,19 +1050,21 @@ DGB_API int dgb_version(void) { return 1; }
 // Kernel timing of the calling thread: enable/disable (clears the totals on
 // enable) and read the per-kind totals (fwd_h, fwd_e, adj_e, adj_h, image).
 DGB_API void dgb_profile(int enable) {
-  g_prof.on = enable != 0;
-  if (g_prof.on)
+  std::lock_guard<std::mutex> lock(g_prof.mu);
+  if (enable)
     for (int k = 0; k < KK_COUNT; ++k) {
       g_prof.ms[k] = 0.0;
       g_prof.launches[k] = 0;
     }
+  g_prof.on = enable != 0;
 }
 
-// Number of kernels this thread has launched through the library so far
+// Time-step kernels launched through the library so far, all threads
 // (graph replays count every kernel node).
-DGB_API long long dgb_launch_count(void) { return g_launch_count; }
+DGB_API long long dgb_launch_count(void) { return g_launch_count.load(); }
 
 DGB_API int dgb_profile_read(double* ms, long long* launches, int n) {
+  std::lock_guard<std::mutex> lock(g_prof.mu);
   const int m = n < KK_COUNT ? n : KK_COUNT;
   for (int k = 0; k < m; ++k) {
     ms[k] = g_prof.ms[k];

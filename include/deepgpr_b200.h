@@ -138,14 +138,14 @@ long long dgb_history_bytes(int kind, int ncomp, int nt_saved, int nshot, long l
 void dgb_forward_f64(/* forward's parameters, float -> double */);
 void dgb_backward_f64(/* backward's parameters, float -> double */);
 
-/* Kernel timing of the calling thread (CUDA events around every time-step
+/* Process-wide kernel timing (CUDA events around every time-step
  * kernel; graph replay is off while enabled).  dgb_profile(1) clears the
  * totals; dgb_profile_read fills ms[k] and launches[k] for the kinds
  * 0 forward-H, 1 forward-E, 2 adjoint-E, 3 adjoint-H, 4 imaging condition,
  * and returns the number of kinds (5). */
 void dgb_profile(int enable);
 int dgb_profile_read(double* ms, long long* launches, int n);
-/* Time-step kernels this thread has launched (graph replays included). */
+/* Time-step kernels launched by the library, all threads (graph replays included). */
 long long dgb_launch_count(void);
 
 #ifdef __cplusplus
