@@ -18,7 +18,7 @@ PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 OUT = PKG / "lib" / "libdeepgpr_b200.so"
 SOURCES = ("fdtd_api.cu",)
-HEADERS = ("fdtd_common.cuh", "fdtd_forward.cuh", "fdtd_adjoint.cuh", "fdtd_tiled.cuh", "fdtd_tiled_adj.cuh")
+HEADERS = ("fdtd_common.cuh", "fdtd_forward.cuh", "fdtd_adjoint.cuh", "fdtd_tiled.cuh", "fdtd_tiled_adj.cuh", "fdtd_tm2d.cuh")
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -86,6 +86,24 @@ __device__ __forceinline__ T pml_weight(T lam, T inv_h, T up, T sign, const Prof
 
 // Transpose of d_back gathered at target coordinate c (deepgpr_cpu.c:429-467).
 // W(d) returns the channel weight of the source point at offset d.
+// Full-radius form: every source point of the target is inside the grid.
+template <typename T, int R, typename WF>
+__device__ __forceinline__ T gather_back_full(const WF& W) {
+  if (R == 1) {
+    T acc = W(0);
+    acc -= W(1);
+    return acc;
+  }
+  T acc = T(0);
+#pragma unroll
+  for (int r = 1; r <= R; ++r) {
+    const T t = tap<T>(R, r);
+    acc += t * W(-(r - 1));
+    acc -= t * W(r);
+  }
+  return acc;
+}
+
 template <typename T, int R, typename WF>
 __device__ __forceinline__ T gather_back(const WF& W, int c, int n) {
   if (R == 1) {
@@ -93,16 +111,8 @@ __device__ __forceinline__ T gather_back(const WF& W, int c, int n) {
     if (c + 1 < n) acc -= W(1);
     return acc;
   }
+  if (c >= 2 * R - 1 && c + 2 * R - 1 < n) return gather_back_full<T, R>(W);
   T acc = T(0);
-  if (c >= 2 * R - 1 && c + 2 * R - 1 < n) {
-#pragma unroll
-    for (int r = 1; r <= R; ++r) {
-      const T t = tap<T>(R, r);
-      acc += t * W(-(r - 1));
-      acc -= t * W(r);
-    }
-    return acc;
-  }
 #pragma unroll
   for (int r = 1; r <= R; ++r) {
     const int up = c - (r - 1);
@@ -121,6 +131,24 @@ __device__ __forceinline__ T gather_back(const WF& W, int c, int n) {
 
 // Transpose of d_fwd gathered at target coordinate c (deepgpr_cpu.c:470-507).
 template <typename T, int R, typename WF>
+__device__ __forceinline__ T gather_fwd_full(const WF& W) {
+  if (R == 1) {
+    T acc = T(0);
+    acc += W(-1);
+    acc -= W(0);
+    return acc;
+  }
+  T acc = T(0);
+#pragma unroll
+  for (int r = 1; r <= R; ++r) {
+    const T t = tap<T>(R, r);
+    acc += t * W(-r);
+    acc -= t * W(r - 1);
+  }
+  return acc;
+}
+
+template <typename T, int R, typename WF>
 __device__ __forceinline__ T gather_fwd(const WF& W, int c, int n) {
   if (R == 1) {
     T acc = T(0);
@@ -128,16 +156,8 @@ __device__ __forceinline__ T gather_fwd(const WF& W, int c, int n) {
     acc -= W(0);
     return acc;
   }
+  if (c >= 2 * R - 1 && c + 2 * R <= n) return gather_fwd_full<T, R>(W);
   T acc = T(0);
-  if (c >= 2 * R - 1 && c + 2 * R <= n) {
-#pragma unroll
-    for (int r = 1; r <= R; ++r) {
-      const T t = tap<T>(R, r);
-      acc += t * W(-r);
-      acc -= t * W(r - 1);
-    }
-    return acc;
-  }
 #pragma unroll
   for (int r = 1; r <= R; ++r) {
     const int up = c - r;

@@ -18,10 +18,11 @@
 #include <cstring>
 #include <atomic>
 #include <mutex>
+#include <type_traits>
 #include <string>
 #include <vector>
 
-#include "fdtd_tiled_adj.cuh"
+#include "fdtd_tm2d.cuh"
 
 #define DGB_API extern "C" __attribute__((visibility("default")))
 
@@ -64,19 +65,27 @@ ProfileState g_prof;
 thread_local std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> g_pending;
 std::atomic<long long> g_launch_count{0};   // time-step kernels launched by the library
 
-// Launch `fn` (which enqueues one kernel on st), timing it when profiling.
+// Launch `fn` (which enqueues one kernel on st, or returns how many kernels
+// it enqueued, all joined back to st), timing it when profiling.
 template <typename F>
 void timed(int kind, cudaStream_t st, F fn) {
-  ++g_launch_count;
+  auto run = [&] {
+    if constexpr (std::is_void_v<decltype(fn())>) {
+      fn();
+      ++g_launch_count;
+    } else {
+      g_launch_count += fn();
+    }
+  };
   if (!g_prof.on) {
-    fn();
+    run();
     return;
   }
   cudaEvent_t a = nullptr, b = nullptr;
   cudaEventCreate(&a);
   cudaEventCreate(&b);
   cudaEventRecord(a, st);
-  fn();
+  run();
   cudaEventRecord(b, st);
   g_pending.push_back({kind, {a, b}});
 }
@@ -116,6 +125,9 @@ struct StreamSet {
   int device = -1;
   cudaStream_t work = nullptr;
   cudaEvent_t in = nullptr, out = nullptr;
+  // side stream: 2D TM frame kernels run on it beside the interior kernels
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
 };
 thread_local std::vector<StreamSet> g_streams;
 
@@ -129,6 +141,9 @@ StreamSet* stream_set() {
   if (cudaStreamCreateWithFlags(&s.work, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
   if (cudaEventCreateWithFlags(&s.in, cudaEventDisableTiming) != cudaSuccess) return nullptr;
   if (cudaEventCreateWithFlags(&s.out, cudaEventDisableTiming) != cudaSuccess) return nullptr;
+  if (cudaStreamCreateWithFlags(&s.side, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
+  if (cudaEventCreateWithFlags(&s.fork, cudaEventDisableTiming) != cudaSuccess) return nullptr;
+  if (cudaEventCreateWithFlags(&s.join, cudaEventDisableTiming) != cudaSuccess) return nullptr;
   g_streams.push_back(s);
   return &g_streams.back();
 }
@@ -223,7 +238,9 @@ bool build_table(const int* loc, int nshot, int npts, const Grid& g, cudaStream_
 
 // Table plus per-shot membership bitmaps.
 bool build_pointset(const int* loc, int nshot, int npts, const Grid& g, cudaStream_t st, Scratch& scratch,
-                    PointSet* ps, PointTable* tb_out, const char* what, int err_code) {
+                    PointSet* ps, PointTable* tb_out, const char* what, int err_code,
+                    const unsigned char** rows_out = nullptr, std::vector<char>* any_rows = nullptr) {
+  if (rows_out) *rows_out = nullptr;
   ps->tb.n = 0;
   ps->tb.cells = ps->tb.off = ps->tb.shot = ps->tb.idx = nullptr;
   ps->bits = nullptr;
@@ -247,10 +264,203 @@ bool build_pointset(const int* loc, int nshot, int npts, const Grid& g, cudaStre
   if (!d) return false;
   if (!cuda_ok(cudaMemcpyAsync(d, bits.data(), bits.size() * sizeof(unsigned), cudaMemcpyHostToDevice, st), what))
     return false;
+  if (any_rows) {
+    // host mask over x indices: some shot has a point there
+    any_rows->assign(g.NX, 0);
+    for (size_t m = 0; m < n; ++m) (*any_rows)[h[m * 3]] = 1;
+  }
+  if (rows_out) {
+    // per (shot, x index) flag: the row/plane holds a point of the shot
+    std::vector<unsigned char> rows((size_t)nshot * g.NX, 0);
+    for (int s = 0; s < nshot; ++s)
+      for (int m = 0; m < npts; ++m) rows[(size_t)s * g.NX + h[((size_t)s * npts + m) * 3]] = 1;
+    unsigned char* dr = scratch.get<unsigned char>(rows.size());
+    if (!dr) return false;
+    if (!cuda_ok(cudaMemcpyAsync(dr, rows.data(), rows.size(), cudaMemcpyHostToDevice, st), what)) return false;
+    if (!cuda_ok(cudaStreamSynchronize(st), what)) return false;
+    *rows_out = dr;
+  }
   if (!cuda_ok(cudaStreamSynchronize(st), what)) return false;
   ps->bits = d;
   return true;
 }
+
+// Strip layout of the 2D TM path: padded pitch and 32-column strips; the
+// rectangles and row chunking of each launch are set by tm_plan.
+TmGeom tm_layout(const Grid& g) {
+  TmGeom tg;
+  memset(&tg, 0, sizeof(tg));
+  tg.NYP = (g.NY + TMW - 1) / TMW * TMW;
+  tg.nseg = tg.NYP / TMW;
+  return tg;
+}
+
+int sm_count() {
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return sms;
+}
+
+template <typename K>
+int blocks_per_sm(K kernel) {
+  int blocks = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, 32 * TM_WARPS, 0) != cudaSuccess || blocks < 1) {
+    cudaGetLastError();
+    blocks = 4;
+  }
+  return blocks;
+}
+
+// Appends rectangle (warp strips of `width` columns starting at column
+// 32 * seg0, nseg of them; rows [row0, row1)) with chunks of xc rows.
+void tm_add_rect(TmGeom& tg, int nshot, int seg0, int nseg, int width, int row0, int row1, int xc) {
+  if (nseg <= 0 || row1 <= row0) return;
+  TmRect& r = tg.rect[tg.nrect++];
+  r.seg0 = seg0;
+  r.nseg = nseg;
+  r.width = width;
+  r.row0 = row0;
+  r.row1 = row1;
+  r.xc = std::max(1, std::min(xc, row1 - row0));
+  r.nchunk = (row1 - row0 + r.xc - 1) / r.xc;
+  r.warp0 = tg.nwarps;
+  tg.nwarps += (long long)nseg * r.nchunk * nshot;
+}
+
+// Interior rectangle of one 2D TM half step and the frame of general work
+// around it.  Interior rows: the longest run where tm_lean_ok holds; interior
+// columns: the longest run of whole 32-column tiles where it holds (so each
+// FP8 scale tile is written by one kernel).  The interior kernels use
+// 64-column strips starting at the first interior column, chunked so a launch
+// is about one wave of resident warps (occupancy `iblocks` CTAs per SM,
+// chunks of at least 16 rows); the frame (32-column strips) uses 8-row chunks,
+// its work being latency-bound.
+struct TmPlan {
+  TmGeom interior, frame;
+};
+
+TmPlan tm_plan(const TmGeom& base, const Grid& g, int kind, int R, const TmFaces& f, bool lean, int iblocks,
+               const std::vector<char>* avoid = nullptr) {
+  TmPlan pl;
+  pl.interior = base;
+  pl.frame = base;
+  // interior row runs: tm_lean_ok rows that hold no source / receiver of any shot
+  std::vector<std::pair<int, int>> runs;
+  int tlo = 0, thi = 0;
+  if (lean) {
+    int cur = -1;
+    for (int i = 0; i <= g.NX; ++i) {
+      const bool y = i < g.NX && tm_lean_ok(kind, 0, i, g.NX, R, f) && !(avoid && !avoid->empty() && (*avoid)[i]);
+      if (y && cur < 0) cur = i;
+      if (!y && cur >= 0) {
+        runs.push_back({cur, i});
+        cur = -1;
+      }
+    }
+    // at most 4 interior runs (the longest), kept in row order
+    if (runs.size() > 4) {
+      std::sort(runs.begin(), runs.end(),
+                [](const std::pair<int, int>& x, const std::pair<int, int>& y) { return x.second - x.first > y.second - y.first; });
+      runs.resize(4);
+      std::sort(runs.begin(), runs.end());
+    }
+    cur = -1;
+    for (int q = 0; q <= base.nseg; ++q) {
+      bool y = q < base.nseg;
+      for (int j = q * TMW; y && j < (q + 1) * TMW; ++j) y = tm_lean_ok(kind, 1, j, g.NY, R, f);
+      if (y && cur < 0) cur = q;
+      if (!y && cur >= 0) {
+        if (q - cur > thi - tlo) {
+          tlo = cur;
+          thi = q;
+        }
+        cur = -1;
+      }
+    }
+  }
+  const int frame_xc = 8;
+  if (!runs.empty() && thi > tlo) {
+    const int n64 = (thi - tlo + 1) / 2;
+    int rows = 0;
+    for (auto& r : runs) rows += r.second - r.first;
+    const long long per = (long long)n64 * g.nshot;
+    const long long resident = (long long)sm_count() * iblocks * TM_WARPS;
+    long long chunks = std::max<long long>(1, resident / per);
+    chunks = std::min<long long>(chunks, std::max(1, rows / 16));
+    const int xc = (int)((rows + chunks - 1) / chunks);
+    for (auto& r : runs) tm_add_rect(pl.interior, g.nshot, tlo, n64, 2 * TMW, r.first, r.second, xc);
+    pl.interior.col1 = thi * TMW;
+    tm_add_rect(pl.frame, g.nshot, 0, tlo, TMW, 0, g.NX, frame_xc);
+    tm_add_rect(pl.frame, g.nshot, thi, base.nseg - thi, TMW, 0, g.NX, frame_xc);
+    int prev = 0;
+    for (auto& r : runs) {
+      tm_add_rect(pl.frame, g.nshot, tlo, thi - tlo, TMW, prev, r.first, frame_xc);
+      prev = r.second;
+    }
+    tm_add_rect(pl.frame, g.nshot, tlo, thi - tlo, TMW, prev, g.NX, frame_xc);
+  } else {
+    tm_add_rect(pl.frame, g.nshot, 0, base.nseg, TMW, 0, g.NX, frame_xc);
+  }
+  return pl;
+}
+
+// 2D imaging kernel for the call's history format.
+template <typename T, int KIND>
+void launch_tm_image_k(bool e_only, bool acc64, unsigned blocks, cudaStream_t st, const AdjArgs<T>& a, const T* lam,
+                       const TmGeom& tg) {
+  if (e_only) {
+    if (acc64) tm_image<T, KIND, true, true><<<blocks, 256, 0, st>>>(a, lam, tg.NYP, tg.nseg);
+    else tm_image<T, KIND, true, false><<<blocks, 256, 0, st>>>(a, lam, tg.NYP, tg.nseg);
+  } else {
+    if (acc64) tm_image<T, KIND, false, true><<<blocks, 256, 0, st>>>(a, lam, tg.NYP, tg.nseg);
+    else tm_image<T, KIND, false, false><<<blocks, 256, 0, st>>>(a, lam, tg.NYP, tg.nseg);
+  }
+}
+
+template <typename T>
+void launch_tm_image(int kind, bool e_only, bool acc64, unsigned blocks, cudaStream_t st, const AdjArgs<T>& a,
+                     const T* lam, const TmGeom& tg) {
+  if constexpr (sizeof(T) == 8) {
+    launch_tm_image_k<T, kF64>(e_only, acc64, blocks, st, a, lam, tg);
+  } else {
+    if (kind == kF16) launch_tm_image_k<T, kF16>(e_only, acc64, blocks, st, a, lam, tg);
+    else if (kind == kBF16) launch_tm_image_k<T, kBF16>(e_only, acc64, blocks, st, a, lam, tg);
+    else if (kind == kFP8) launch_tm_image_k<T, kFP8>(e_only, acc64, blocks, st, a, lam, tg);
+    else launch_tm_image_k<T, kF32>(e_only, acc64, blocks, st, a, lam, tg);
+  }
+}
+
+// One 2D TM half step: the frame kernel on the side stream, forked from and
+// joined back to st, beside the interior kernel on st.  Returns the number
+// of kernels launched.
+template <typename FrameFn, typename InteriorFn>
+int split_launch(cudaStream_t st, const StreamSet* ss, bool has_interior, FrameFn frame, InteriorFn interior) {
+  if (!has_interior || ss == nullptr || ss->side == nullptr) {
+    frame(st);
+    if (has_interior) interior(st);
+    return has_interior ? 2 : 1;
+  }
+  cudaEventRecord(ss->fork, st);
+  cudaStreamWaitEvent(ss->side, ss->fork, 0);
+  frame(ss->side);
+  cudaEventRecord(ss->join, ss->side);
+  interior(st);
+  cudaStreamWaitEvent(st, ss->join, 0);
+  return 2;
+}
+
+template <typename T>
+TmFaces tm_faces(const Face<T>* eF, const Face<T>* hF, bool cpml) {
+  TmFaces f;
+  memset(&f, 0, sizeof(f));
+  if (cpml) {
+    f.hx0 = hF[0].p; f.hx1 = hF[1].p; f.hy0 = hF[2].p; f.hy1 = hF[3].p;
+    f.ex0 = eF[0].p; f.ex1 = eF[1].p; f.ey0 = eF[2].p; f.ey1 = eF[3].p;
+  }
+  return f;
+}
+
+dim3 tm_grid(const TmGeom& tg) { return dim3((unsigned)std::max<long long>(1, (tg.nwarps + TM_WARPS - 1) / TM_WARPS)); }
 
 // x-chunk length that gives about 8 resident CTAs per SM.
 int pick_xchunk(int NX, long long tiles_per_plane, int nshot, int min_chunk) {
@@ -266,7 +476,6 @@ int pick_xchunk(int NX, long long tiles_per_plane, int nshot, int min_chunk) {
 }
 
 long long tiles3(const Grid& g) { return (long long)((g.NY + TY - 1) / TY) * ((g.NZ + TZ - 1) / TZ); }
-long long tiles2(const Grid& g) { return (long long)(g.NY + T2 - 1) / T2; }
 
 template <typename T>
 __global__ void k_coeffs(const T* __restrict__ eps, const T* __restrict__ sig, const T* __restrict__ mu,
@@ -326,9 +535,10 @@ HBox make_box(const Grid& g, bool physical, const int* p) {
 
 long long ntiles_of(const Grid& g) { return ((long long)g.cells + kBlock - 1) / kBlock; }
 
-// FP8 scale tiles: one per (x plane, CTA tile) of the forward kernels.
+// FP8 scale tiles: one per (x plane, CTA tile) of the 3D forward kernels, one
+// per (row, 32-column strip) of the 2D TM kernels.
 long long fp8_tiles(const Grid& g, bool tm2d) {
-  return (long long)g.NX * (tm2d ? (long long)(g.NY + T2 - 1) / T2
+  return (long long)g.NX * (tm2d ? (long long)(g.NY + TMW - 1) / TMW
                                  : (long long)((g.NY + TY - 1) / TY) * ((g.NZ + TZ - 1) / TZ));
 }
 
@@ -536,14 +746,26 @@ void forward_impl(const ForwardCall<T>& fc) {
     }
     Control* ctrl = scratch.get<Control>(sizeof(Control));
     ok = !scratch.failed;
+    const int R = radius_of(g_opt.order_override ? g_opt.order_override : g_order);
+    TmGeom tg;
+    memset(&tg, 0, sizeof(tg));
+    if (tm2d) tg = tm_layout(g);
     // sources of an invalid component inject nothing (deepgpr_cpu.c:650)
+    std::vector<char> src_any, rcv_any;
     if (ok && fc.src_comp >= 0 && fc.src_comp <= 2)
-      ok = build_pointset(fc.src_loc, g.nshot, fc.nsrc, g, st, scratch, &P.src, &a.src, "source", kErrSourceRange);
-    if (ok) ok = build_pointset(fc.rx_loc, g.nshot, fc.nrx, g, st, scratch, &P.rcv, &a.rcv, "receiver", kErrReceiverRange);
+      ok = build_pointset(fc.src_loc, g.nshot, fc.nsrc, g, st, scratch, &P.src, &a.src, "source", kErrSourceRange,
+                          tm2d ? &tg.src_rows : nullptr, tm2d ? &src_any : nullptr);
+    if (ok)
+      ok = build_pointset(fc.rx_loc, g.nshot, fc.nrx, g, st, scratch, &P.rcv, &a.rcv, "receiver", kErrReceiverRange,
+                          tm2d ? &tg.rcv_rows : nullptr, tm2d ? &rcv_any : nullptr);
+    // rows with a source or receiver of any shot go to the general (frame) kernels
+    std::vector<char> pt_rows(tm2d ? g.NX : 0, 0);
+    for (int i = 0; i < (int)pt_rows.size(); ++i)
+      pt_rows[i] = (i < (int)src_any.size() && src_any[i]) || (i < (int)rcv_any.size() && rcv_any[i]);
     if (ok) ok = launch_coeffs(cm, st);
-    TmFields<T> tf;
+    TmBuf<T> tf;
     memset(&tf, 0, sizeof(tf));
-    const long long plane2 = (long long)g.NX * g.NY;
+    const long long plane2 = (long long)g.NX * tg.NYP;
     if (ok && tm2d) {
       T* buf = scratch.get<T>((size_t)(3 * g.nshot + 5) * plane2 * sizeof(T));
       ok = buf != nullptr;
@@ -553,39 +775,73 @@ void forward_impl(const ForwardCall<T>& fc) {
         tf.Hy = buf + 2 * g.nshot * plane2;
         T* cf = buf + 3 * g.nshot * plane2;
         const T* srcs[5] = {cm.ce_hist, cm.ce_curl, cm.ce_rhs, cm.ch_curl, cm.ch_rhs};
-        for (int q = 0; q < 5; ++q) k_pack2d<T><<<1024, 256, 0, st>>>(srcs[q], cf + q * plane2, plane2);
+        for (int q = 0; q < 5; ++q) k_pack2d_pitch<T><<<1024, 256, 0, st>>>(srcs[q], cf + q * plane2, g.NX, g.NY, tg.NYP);
         tf.ce_hist = cf;
         tf.ce_curl = cf + plane2;
         tf.ce_rhs = cf + 2 * plane2;
         tf.ch_curl = cf + 3 * plane2;
         tf.ch_rhs = cf + 4 * plane2;
-        k_pack2d<T><<<2048, 256, 0, st>>>(fc.Ez, tf.Ez, g.nshot * plane2);
-        k_pack2d<T><<<2048, 256, 0, st>>>(fc.Hx, tf.Hx, g.nshot * plane2);
-        k_pack2d<T><<<2048, 256, 0, st>>>(fc.Hy, tf.Hy, g.nshot * plane2);
+        k_pack2d_pitch<T><<<2048, 256, 0, st>>>(fc.Ez, tf.Ez, (long long)g.nshot * g.NX, g.NY, tg.NYP);
+        k_pack2d_pitch<T><<<2048, 256, 0, st>>>(fc.Hx, tf.Hx, (long long)g.nshot * g.NX, g.NY, tg.NYP);
+        k_pack2d_pitch<T><<<2048, 256, 0, st>>>(fc.Hy, tf.Hy, (long long)g.nshot * g.NX, g.NY, tg.NYP);
         ok = cuda_ok(cudaGetLastError(), "pack");
       }
     }
     if (ok) {
       a.ctrl = ctrl;
       k_set<<<1, 1, 0, st>>>(ctrl, 0);
-      const int R = radius_of(g_opt.order_override ? g_opt.order_override : g_order);
-      const long long tiles = tm2d ? tiles2(g) : tiles3(g);
+      const long long tiles = tm2d ? 1 : tiles3(g);
       P.xchunk = pick_xchunk(g.NX, tiles, g.nshot, 4 * R);
       P.tm2d = tm2d;
       dim3 grid((unsigned)tiles, (unsigned)((g.NX + P.xchunk - 1) / P.xchunk), (unsigned)g.nshot);
+      const dim3 wblock(32, TM_WARPS);
+      // 2D TM: general kernels on the CPML / boundary frame, interior kernels inside
+      const bool lean2d = tm2d && a.box.z0 == 0 && a.box.nz == 1;
+      const TmFaces tfc = tm_faces(a.eF, a.hF, a.has_cpml != 0);
+      TmPlan pH, pE;
+      if (tm2d) {
+        const int bH = R == 1 ? blocks_per_sm(tmi_fwd_h<T, 1>) : R == 2 ? blocks_per_sm(tmi_fwd_h<T, 2>)
+                                                                        : blocks_per_sm(tmi_fwd_h<T, 4>);
+        const int bE = R == 1 ? blocks_per_sm(tmi_fwd_e<T, 1>) : R == 2 ? blocks_per_sm(tmi_fwd_e<T, 2>)
+                                                                        : blocks_per_sm(tmi_fwd_e<T, 4>);
+        pH = tm_plan(tg, g, 0, R, tfc, lean2d, bH);
+        pE = tm_plan(tg, g, 1, R, tfc, lean2d, bE, &pt_rows);
+      }
       auto issue = [&](int k) {
         TiledFwd<T> b = P;
         b.a.k_in_chunk = k;
         if (tm2d) {
           timed(KK_FWD_H, st, [&] {
-            if (R == 1) k2_fwd_h<T, 1><<<grid, T2, 0, st>>>(b, tf);
-            else if (R == 2) k2_fwd_h<T, 2><<<grid, T2, 0, st>>>(b, tf);
-            else k2_fwd_h<T, 4><<<grid, T2, 0, st>>>(b, tf);
+            return split_launch(
+                st, ss, pH.interior.nwarps > 0,
+                [&](cudaStream_t q) {
+                  const dim3 gf = tm_grid(pH.frame);
+                  if (R == 1) tm_fwd_h<T, 1><<<gf, wblock, 0, q>>>(b, tf, pH.frame);
+                  else if (R == 2) tm_fwd_h<T, 2><<<gf, wblock, 0, q>>>(b, tf, pH.frame);
+                  else tm_fwd_h<T, 4><<<gf, wblock, 0, q>>>(b, tf, pH.frame);
+                },
+                [&](cudaStream_t q) {
+                  const dim3 gi = tm_grid(pH.interior);
+                  if (R == 1) tmi_fwd_h<T, 1><<<gi, wblock, 0, q>>>(b, tf, pH.interior);
+                  else if (R == 2) tmi_fwd_h<T, 2><<<gi, wblock, 0, q>>>(b, tf, pH.interior);
+                  else tmi_fwd_h<T, 4><<<gi, wblock, 0, q>>>(b, tf, pH.interior);
+                });
           });
           timed(KK_FWD_E, st, [&] {
-            if (R == 1) k2_fwd_e<T, 1><<<grid, T2, 0, st>>>(b, tf);
-            else if (R == 2) k2_fwd_e<T, 2><<<grid, T2, 0, st>>>(b, tf);
-            else k2_fwd_e<T, 4><<<grid, T2, 0, st>>>(b, tf);
+            return split_launch(
+                st, ss, pE.interior.nwarps > 0,
+                [&](cudaStream_t q) {
+                  const dim3 gf = tm_grid(pE.frame);
+                  if (R == 1) tm_fwd_e<T, 1><<<gf, wblock, 0, q>>>(b, tf, pE.frame);
+                  else if (R == 2) tm_fwd_e<T, 2><<<gf, wblock, 0, q>>>(b, tf, pE.frame);
+                  else tm_fwd_e<T, 4><<<gf, wblock, 0, q>>>(b, tf, pE.frame);
+                },
+                [&](cudaStream_t q) {
+                  const dim3 gi = tm_grid(pE.interior);
+                  if (R == 1) tmi_fwd_e<T, 1><<<gi, wblock, 0, q>>>(b, tf, pE.interior);
+                  else if (R == 2) tmi_fwd_e<T, 2><<<gi, wblock, 0, q>>>(b, tf, pE.interior);
+                  else tmi_fwd_e<T, 4><<<gi, wblock, 0, q>>>(b, tf, pE.interior);
+                });
           });
         } else {
           timed(KK_FWD_H, st, [&] {
@@ -602,9 +858,9 @@ void forward_impl(const ForwardCall<T>& fc) {
       };
       ok = run_loop(cm.nt, +1, ctrl, st, issue);
       if (ok && tm2d) {
-        k_unpack2d<T><<<2048, 256, 0, st>>>(tf.Ez, fc.Ez, g.nshot * plane2);
-        k_unpack2d<T><<<2048, 256, 0, st>>>(tf.Hx, fc.Hx, g.nshot * plane2);
-        k_unpack2d<T><<<2048, 256, 0, st>>>(tf.Hy, fc.Hy, g.nshot * plane2);
+        k_unpack2d_pitch<T><<<2048, 256, 0, st>>>(tf.Ez, fc.Ez, (long long)g.nshot * g.NX, g.NY, tg.NYP);
+        k_unpack2d_pitch<T><<<2048, 256, 0, st>>>(tf.Hx, fc.Hx, (long long)g.nshot * g.NX, g.NY, tg.NYP);
+        k_unpack2d_pitch<T><<<2048, 256, 0, st>>>(tf.Hy, fc.Hy, (long long)g.nshot * g.NX, g.NY, tg.NYP);
         ok = cuda_ok(cudaGetLastError(), "unpack");
       }
       if (ok && e_only) {
@@ -805,14 +1061,26 @@ void backward_impl(const BackwardCall<T>& bc) {
         }
       }
     }
+    const int R = radius_of(g_opt.order_override ? g_opt.order_override : g_order);
+    TmGeom tg;
+    memset(&tg, 0, sizeof(tg));
+    if (tm2d) tg = tm_layout(g);
+    std::vector<char> src_any, rcv_any;
     if (ok && a.want_src) {
       a.srcv = scratch.get<T>((size_t)g.nshot * bc.nsrc * sizeof(T));
       ok = a.srcv != nullptr;
       if (ok) cudaMemsetAsync(a.srcv, 0, (size_t)g.nshot * bc.nsrc * sizeof(T), st);
-      if (ok) ok = build_pointset(bc.src_loc, g.nshot, bc.nsrc, g, st, scratch, &P.src, &a.src, "source", kErrSourceRange);
+      if (ok)
+        ok = build_pointset(bc.src_loc, g.nshot, bc.nsrc, g, st, scratch, &P.src, &a.src, "source", kErrSourceRange,
+                            tm2d ? &tg.src_rows : nullptr, tm2d ? &src_any : nullptr);
     }
     if (ok && bc.rx_comp >= 0 && bc.rx_comp <= 2)
-      ok = build_pointset(bc.rx_loc, g.nshot, bc.ndata, g, st, scratch, &P.rcv, &a.rcv, "receiver", kErrReceiverRange);
+      ok = build_pointset(bc.rx_loc, g.nshot, bc.ndata, g, st, scratch, &P.rcv, &a.rcv, "receiver", kErrReceiverRange,
+                          tm2d ? &tg.rcv_rows : nullptr, tm2d ? &rcv_any : nullptr);
+    // rows with a receiver or source of any shot go to the general (frame) kernels
+    std::vector<char> pt_rows(tm2d ? g.NX : 0, 0);
+    for (int i = 0; i < (int)pt_rows.size(); ++i)
+      pt_rows[i] = (i < (int)src_any.size() && src_any[i]) || (i < (int)rcv_any.size() && rcv_any[i]);
     const long long ncell_ext = (long long)(g.NX - 1) * (g.NY - 1) * (g.NZ - 1);
     if (ok && want_model && a.acc64) {
       a.g_eps64 = scratch.get<double>((size_t)ncell_ext * sizeof(double));
@@ -824,49 +1092,62 @@ void backward_impl(const BackwardCall<T>& bc) {
       }
     }
     if (ok) ok = launch_coeffs(cm, st);
-    TmAdj<T> tl;
+    TmBuf<T> tl;
     memset(&tl, 0, sizeof(tl));
-    const long long plane2 = (long long)g.NX * g.NY;
+    const long long plane2 = (long long)g.NX * tg.NYP;
     if (ok && tm2d) {
       T* buf = scratch.get<T>((size_t)(3 * g.nshot + 5) * plane2 * sizeof(T));
       ok = buf != nullptr;
       if (ok) {
-        tl.lEz = buf;
-        tl.lHx = buf + g.nshot * plane2;
-        tl.lHy = buf + 2 * g.nshot * plane2;
+        tl.Ez = buf;
+        tl.Hx = buf + g.nshot * plane2;
+        tl.Hy = buf + 2 * g.nshot * plane2;
         T* cf = buf + 3 * g.nshot * plane2;
         const T* srcs[5] = {cm.ce_hist, cm.ce_curl, cm.ce_rhs, cm.ch_curl, cm.ch_rhs};
-        for (int q = 0; q < 5; ++q) k_pack2d<T><<<1024, 256, 0, st>>>(srcs[q], cf + q * plane2, plane2);
+        for (int q = 0; q < 5; ++q) k_pack2d_pitch<T><<<1024, 256, 0, st>>>(srcs[q], cf + q * plane2, g.NX, g.NY, tg.NYP);
         tl.ce_hist = cf;
         tl.ce_curl = cf + plane2;
         tl.ce_rhs = cf + 2 * plane2;
         tl.ch_curl = cf + 3 * plane2;
         tl.ch_rhs = cf + 4 * plane2;
-        k_pack2d<T><<<2048, 256, 0, st>>>(bc.lEz, tl.lEz, g.nshot * plane2);
-        k_pack2d<T><<<2048, 256, 0, st>>>(bc.lHx, tl.lHx, g.nshot * plane2);
-        k_pack2d<T><<<2048, 256, 0, st>>>(bc.lHy, tl.lHy, g.nshot * plane2);
+        k_pack2d_pitch<T><<<2048, 256, 0, st>>>(bc.lEz, tl.Ez, (long long)g.nshot * g.NX, g.NY, tg.NYP);
+        k_pack2d_pitch<T><<<2048, 256, 0, st>>>(bc.lHx, tl.Hx, (long long)g.nshot * g.NX, g.NY, tg.NYP);
+        k_pack2d_pitch<T><<<2048, 256, 0, st>>>(bc.lHy, tl.Hy, (long long)g.nshot * g.NX, g.NY, tg.NYP);
         ok = cuda_ok(cudaGetLastError(), "pack");
       }
     }
     if (ok && cm.nt > 0) {
       a.ctrl = ctrl;
       k_set<<<1, 1, 0, st>>>(ctrl, cm.nt - 1);
-      const int R = radius_of(g_opt.order_override ? g_opt.order_override : g_order);
-      const long long tiles = tm2d ? tiles2(g) : tiles3(g);
+      const long long tiles = tm2d ? 1 : tiles3(g);
+      const dim3 wblock(32, TM_WARPS);
+      const bool lean2d = tm2d && a.box.z0 == 0 && a.box.nz == 1;
+      const TmFaces tfc = tm_faces(a.eF, a.hF, a.has_cpml != 0);
+      TmPlan pE, pH, pP;
+      if (tm2d) {
+        const int bE = R == 1 ? blocks_per_sm(tmi_adj_e<T, 1>) : R == 2 ? blocks_per_sm(tmi_adj_e<T, 2>)
+                                                                        : blocks_per_sm(tmi_adj_e<T, 4>);
+        const int bH = R == 1 ? blocks_per_sm(tmi_adj_h<T, 1>) : R == 2 ? blocks_per_sm(tmi_adj_h<T, 2>)
+                                                                        : blocks_per_sm(tmi_adj_h<T, 4>);
+        pE = tm_plan(tg, g, 2, R, tfc, lean2d, bE);
+        pH = tm_plan(tg, g, 3, R, tfc, lean2d, bH, &pt_rows);
+        pP = tm_plan(tg, g, 3, R, tfc, false, bH);   // prologue: general kernel everywhere
+      }
       P.xchunk = pick_xchunk(g.NX, tiles, g.nshot, 4 * R);
       dim3 grid((unsigned)tiles, (unsigned)((g.NX + P.xchunk - 1) / P.xchunk), (unsigned)g.nshot);
       const unsigned img_blocks = (unsigned)((a.box.cells() + 255) / 256);
-      const T* lamx = tm2d ? tl.lEz : bc.lEx;
-      const T* lamy = tm2d ? tl.lEz : bc.lEy;
-      const T* lamz = tm2d ? tl.lEz : bc.lEz;
+      const T* lamx = bc.lEx;
+      const T* lamy = bc.lEy;
+      const T* lamz = bc.lEz;
       // head of step nt-1
       {
         TiledAdj<T> b = P;
         b.a.k_in_chunk = 0;
         if (tm2d) {
-          if (R == 1) k2_adj_h<T, 1, true><<<grid, T2, 0, st>>>(b, tl);
-          else if (R == 2) k2_adj_h<T, 2, true><<<grid, T2, 0, st>>>(b, tl);
-          else k2_adj_h<T, 4, true><<<grid, T2, 0, st>>>(b, tl);
+          const dim3 gP = tm_grid(pP.frame);
+          if (R == 1) tm_adj_h<T, 1, true><<<gP, wblock, 0, st>>>(b, tl, pP.frame);
+          else if (R == 2) tm_adj_h<T, 2, true><<<gP, wblock, 0, st>>>(b, tl, pP.frame);
+          else tm_adj_h<T, 4, true><<<gP, wblock, 0, st>>>(b, tl, pP.frame);
         } else {
           if (R == 1) k3_adj_h<T, 1, true><<<grid, 256, 0, st>>>(b);
           else if (R == 2) k3_adj_h<T, 2, true><<<grid, 256, 0, st>>>(b);
@@ -877,18 +1158,44 @@ void backward_impl(const BackwardCall<T>& bc) {
       auto issue = [&](int k) {
         TiledAdj<T> b = P;
         b.a.k_in_chunk = k;
-        if (want_model && img_blocks > 0)
-          timed(KK_IMAGE, st, [&] { k_image<T><<<img_blocks, 256, 0, st>>>(b.a, lamx, lamy, lamz, tm2d ? 1 : 0); });
+        if (want_model && img_blocks > 0) {
+          if (tm2d)
+            timed(KK_IMAGE, st, [&] { launch_tm_image<T>(kind, a.e_only != 0, a.acc64 != 0, img_blocks, st, b.a, tl.Ez, tg); });
+          else
+            timed(KK_IMAGE, st, [&] { k_image<T><<<img_blocks, 256, 0, st>>>(b.a, lamx, lamy, lamz); });
+        }
         if (tm2d) {
           timed(KK_ADJ_E, st, [&] {
-            if (R == 1) k2_adj_e<T, 1><<<grid, T2, 0, st>>>(b, tl);
-            else if (R == 2) k2_adj_e<T, 2><<<grid, T2, 0, st>>>(b, tl);
-            else k2_adj_e<T, 4><<<grid, T2, 0, st>>>(b, tl);
+            return split_launch(
+                st, ss, pE.interior.nwarps > 0,
+                [&](cudaStream_t q) {
+                  const dim3 gf = tm_grid(pE.frame);
+                  if (R == 1) tm_adj_e<T, 1><<<gf, wblock, 0, q>>>(b, tl, pE.frame);
+                  else if (R == 2) tm_adj_e<T, 2><<<gf, wblock, 0, q>>>(b, tl, pE.frame);
+                  else tm_adj_e<T, 4><<<gf, wblock, 0, q>>>(b, tl, pE.frame);
+                },
+                [&](cudaStream_t q) {
+                  const dim3 gi = tm_grid(pE.interior);
+                  if (R == 1) tmi_adj_e<T, 1><<<gi, wblock, 0, q>>>(b, tl, pE.interior);
+                  else if (R == 2) tmi_adj_e<T, 2><<<gi, wblock, 0, q>>>(b, tl, pE.interior);
+                  else tmi_adj_e<T, 4><<<gi, wblock, 0, q>>>(b, tl, pE.interior);
+                });
           });
           timed(KK_ADJ_H, st, [&] {
-            if (R == 1) k2_adj_h<T, 1, false><<<grid, T2, 0, st>>>(b, tl);
-            else if (R == 2) k2_adj_h<T, 2, false><<<grid, T2, 0, st>>>(b, tl);
-            else k2_adj_h<T, 4, false><<<grid, T2, 0, st>>>(b, tl);
+            return split_launch(
+                st, ss, pH.interior.nwarps > 0,
+                [&](cudaStream_t q) {
+                  const dim3 gf = tm_grid(pH.frame);
+                  if (R == 1) tm_adj_h<T, 1, false><<<gf, wblock, 0, q>>>(b, tl, pH.frame);
+                  else if (R == 2) tm_adj_h<T, 2, false><<<gf, wblock, 0, q>>>(b, tl, pH.frame);
+                  else tm_adj_h<T, 4, false><<<gf, wblock, 0, q>>>(b, tl, pH.frame);
+                },
+                [&](cudaStream_t q) {
+                  const dim3 gi = tm_grid(pH.interior);
+                  if (R == 1) tmi_adj_h<T, 1><<<gi, wblock, 0, q>>>(b, tl, pH.interior);
+                  else if (R == 2) tmi_adj_h<T, 2><<<gi, wblock, 0, q>>>(b, tl, pH.interior);
+                  else tmi_adj_h<T, 4><<<gi, wblock, 0, q>>>(b, tl, pH.interior);
+                });
           });
         } else {
           timed(KK_ADJ_E, st, [&] {
@@ -905,9 +1212,9 @@ void backward_impl(const BackwardCall<T>& bc) {
       };
       if (ok) ok = run_loop(cm.nt, -1, ctrl, st, issue);
       if (ok && tm2d) {
-        k_unpack2d<T><<<2048, 256, 0, st>>>(tl.lEz, bc.lEz, g.nshot * plane2);
-        k_unpack2d<T><<<2048, 256, 0, st>>>(tl.lHx, bc.lHx, g.nshot * plane2);
-        k_unpack2d<T><<<2048, 256, 0, st>>>(tl.lHy, bc.lHy, g.nshot * plane2);
+        k_unpack2d_pitch<T><<<2048, 256, 0, st>>>(tl.Ez, bc.lEz, (long long)g.nshot * g.NX, g.NY, tg.NYP);
+        k_unpack2d_pitch<T><<<2048, 256, 0, st>>>(tl.Hx, bc.lHx, (long long)g.nshot * g.NX, g.NY, tg.NYP);
+        k_unpack2d_pitch<T><<<2048, 256, 0, st>>>(tl.Hy, bc.lHy, (long long)g.nshot * g.NX, g.NY, tg.NYP);
         ok = cuda_ok(cudaGetLastError(), "unpack");
       }
       if (ok && want_model && a.acc64) {

@@ -146,9 +146,9 @@ __device__ __forceinline__ bool upd_hz(const Grid& g, int i, int j, int k) {
 }
 
 // CPML slab position q on a face, or -1 (deepgpr_cpu.c:754-760, 965-971).
-__device__ __forceinline__ int q_low_e(int p, int c) { return (p > 0 && c > 0 && c <= p) ? p - c : -1; }
-__device__ __forceinline__ int q_low_h(int p, int c) { return (p > 0 && c < p) ? p - 1 - c : -1; }
-__device__ __forceinline__ int q_high(int p, int c, int n) {
+__host__ __device__ __forceinline__ int q_low_e(int p, int c) { return (p > 0 && c > 0 && c <= p) ? p - c : -1; }
+__host__ __device__ __forceinline__ int q_low_h(int p, int c) { return (p > 0 && c < p) ? p - 1 - c : -1; }
+__host__ __device__ __forceinline__ int q_high(int p, int c, int n) {
   return (p > 0 && c >= n - 1 - p && c < n - 1) ? c - (n - 1 - p) : -1;
 }
 

@@ -7,10 +7,7 @@
 // plane from double-buffered shared memory with an R-cell halo (coalesced
 // loads, the halo comes from L2).  One __syncthreads per plane.
 //
-// 2D TM (nz = 1, Ez/Hx/Hy only): fields live in a compact (shot, NX, NY)
-// layout inside a call (the ABI layout interleaves the unused k = 1 halo and
-// would waste half of every sector); a CTA owns 128 consecutive columns and
-// streams along x the same way.
+// The 2D TM path (nz = 1, Ez/Hx/Hy only) has its own kernels in fdtd_tm2d.cuh.
 //
 // Per-cell arithmetic is identical to the reference order (see
 // fdtd_forward.cuh for the line references); only where the operands come
@@ -22,18 +19,31 @@
 namespace dg {
 
 constexpr int TZ = 32, TY = 8;       // 3D tile (threads = 256)
-constexpr int T2 = 128;              // 2D TM tile (threads)
 
 // Stencils on an accessor f(d) = value at offset d along the axis.
+// Full-radius forms (the stencil lies inside the grid).
+template <typename T, int R, typename F>
+__device__ __forceinline__ T dfwd_full(const F& f) {
+  if (R == 1) return f(1) - f(0);
+  T acc = T(0);
+#pragma unroll
+  for (int r = 1; r <= R; ++r) acc += tap<T>(R, r) * (f(r) - f(-(r - 1)));
+  return acc;
+}
+template <typename T, int R, typename F>
+__device__ __forceinline__ T dback_full(const F& f) {
+  if (R == 1) return f(0) - f(-1);
+  T acc = T(0);
+#pragma unroll
+  for (int r = 1; r <= R; ++r) acc += tap<T>(R, r) * (f(r - 1) - f(-r));
+  return acc;
+}
+
 template <typename T, int R, typename F>
 __device__ __forceinline__ T dfwd_f(const F& f, int c, int n) {
   if (R == 1) return f(1) - f(0);
+  if (c - R + 1 >= 0 && c + R < n) return dfwd_full<T, R>(f);
   T acc = T(0);
-  if (c - R + 1 >= 0 && c + R < n) {
-#pragma unroll
-    for (int r = 1; r <= R; ++r) acc += tap<T>(R, r) * (f(r) - f(-(r - 1)));
-    return acc;
-  }
   const int rr = rad_fwd(c, n, R);
 #pragma unroll
   for (int r = 1; r <= R; ++r)
@@ -44,12 +54,8 @@ __device__ __forceinline__ T dfwd_f(const F& f, int c, int n) {
 template <typename T, int R, typename F>
 __device__ __forceinline__ T dback_f(const F& f, int c, int n) {
   if (R == 1) return f(0) - f(-1);
+  if (c >= R && c + R - 1 < n) return dback_full<T, R>(f);
   T acc = T(0);
-  if (c >= R && c + R - 1 < n) {
-#pragma unroll
-    for (int r = 1; r <= R; ++r) acc += tap<T>(R, r) * (f(r - 1) - f(-r));
-    return acc;
-  }
   const int rr = rad_back(c, n, R);
 #pragma unroll
   for (int r = 1; r <= R; ++r)
@@ -137,10 +143,6 @@ __device__ __forceinline__ void fill_plane(T* s, const T* plane, T own, int own_
 __device__ __forceinline__ long long fp8_tile3(const Grid& g, int i, int j, int k) {
   const int nzt = (g.NZ + TZ - 1) / TZ, nyt = (g.NY + TY - 1) / TY;
   return ((long long)i * nyt + j / TY) * nzt + k / TZ;
-}
-__device__ __forceinline__ long long fp8_tile2(const Grid& g, int i, int j) {
-  const int nyt = (g.NY + T2 - 1) / T2;
-  return (long long)i * nyt + j / T2;
 }
 
 template <typename T>
@@ -524,16 +526,6 @@ __global__ void __launch_bounds__(256) k3_fwd_e(TiledFwd<T> P) {
   }
 }
 
-// ---------------------------------------------------------------------------
-// 2D TM: compact (shot, NX, NY) arrays of Ez, Hx, Hy and of the coefficients.
-// Only Ez, Hx, Hy are advanced (src/DeepGPR/lib/deepgpr.h:74-80).
-// ---------------------------------------------------------------------------
-template <typename T>
-struct TmFields {
-  T *Ez, *Hx, *Hy;                 // (nshot, NX, NY)
-  const T *ce_hist, *ce_curl, *ce_rhs, *ch_curl, *ch_rhs;   // (NX, NY)
-};
-
 // 2D Yee predicates (NZ = 2, k = 0): Ez, Hx, Hy of the general rules.
 __device__ __forceinline__ bool tm_upd_ez(const Grid& g, int i, int j) {
   return (g.NX - 1 != 1 || g.NY - 1 != 1) && i > 0 && i < g.NX - 1 && j > 0 && j < g.NY - 1;
@@ -543,238 +535,6 @@ __device__ __forceinline__ bool tm_upd_hx(const Grid& g, int i, int j) {
 }
 __device__ __forceinline__ bool tm_upd_hy(const Grid& g, int i, int j) {
   return g.NY - 1 != 1 && i < g.NX - 1 && j > 0 && j < g.NY - 1;
-}
-
-template <typename T, int R>
-__global__ void __launch_bounds__(T2) k2_fwd_h(TiledFwd<T> P, TmFields<T> f) {
-  constexpr int W = T2 + 2 * R;
-  __shared__ T sEz[2][W];
-  __shared__ float red[33];
-  const FwdArgs<T>& a = P.a;
-  const Grid& g = a.g;
-  const int NX = g.NX, NY = g.NY;
-  const int j0 = blockIdx.x * T2;
-  const int j = j0 + threadIdx.x;
-  const bool colv = j < NY;
-  const int x0 = blockIdx.y * P.xchunk, x1 = min(x0 + P.xchunk, NX);
-  const int s = blockIdx.z;
-  const long long sb = (long long)s * NX * NY;
-  const int it = a.ctrl->cur + a.k_in_chunk;
-  const bool save = a.save_e && (it % a.S == 0);
-  const int slot = it / a.S;
-  const int qy0 = (colv && a.has_cpml) ? q_low_h(a.hF[2].p, j) : -1;
-  const int qy1 = (colv && a.has_cpml) ? q_high(a.hF[3].p, j, NY) : -1;
-  // halo slots: threads 0..R-1 load the left halo, threads R..2R-1 the right one
-  const int hcol = threadIdx.x < R ? j0 - R + (int)threadIdx.x : j0 + T2 + (int)threadIdx.x - R;
-  const bool hload = threadIdx.x < 2 * R && hcol >= 0 && hcol < NY;
-  const int hs = threadIdx.x < R ? (int)threadIdx.x : T2 + (int)threadIdx.x;
-  T q[2 * R];   // Ez at rows i-R+1 .. i+R
-#pragma unroll
-  for (int m = 0; m < 2 * R - 1; ++m) {
-    const int r = x0 - R + 1 + m;
-    q[m] = (colv && r >= 0 && r < NX) ? f.Ez[sb + (long long)r * NY + j] : T(0);
-  }
-  for (int i = x0; i < x1; ++i) {
-    const int b = (i - x0) & 1;
-    {
-      const int r = i + R;
-      q[2 * R - 1] = (colv && r < NX) ? f.Ez[sb + (long long)r * NY + j] : T(0);
-    }
-    const long long rb = sb + (long long)i * NY;
-    sEz[b][R + threadIdx.x] = q[R - 1];
-    if (threadIdx.x < 2 * R) sEz[b][hs] = hload ? f.Ez[rb + hcol] : T(0);
-    __syncthreads();
-    if (save) {
-      long long h = 0;
-      const bool inbox = colv && in_box(a.box, i, j, 0, h);
-      const T v = q[R - 1];
-      float inv = 1.0f;
-      if (a.kind == kFP8) {
-        const float am = block_absmax(inbox ? fabsf(float(v)) : 0.0f, red);
-        const float sc = fp8_scale_of(am);
-        inv = 1.0f / sc;
-        if (threadIdx.x == 0) a.e_scales[((long long)slot * g.nshot + s) * a.ntiles + fp8_tile2(g, i, j0)] = sc;
-      }
-      if (inbox) hist_store<T>(a.E_saved, slot * a.frame + s * a.box.cells() + h, v, a.kind, inv);
-    }
-    if (colv) {
-      const bool dhx = tm_upd_hx(g, i, j), dhy = tm_upd_hy(g, i, j);
-      const int qx0 = a.has_cpml ? q_low_h(a.hF[0].p, i) : -1;
-      const int qx1 = a.has_cpml ? q_high(a.hF[1].p, i, NX) : -1;
-      const bool in_x = qx0 >= 0 || qx1 >= 0, in_y = qy0 >= 0 || qy1 >= 0;
-      const int c = i * NY + j;
-      const T c1 = f.ch_curl[c];
-      const T cy = curl_scale(c1, a.dx, a.dy, a.dy_eq);
-      const T* ez_ = sEz[b];
-      T dEz_dy = T(0), dEz_dx = T(0);
-      if (dhx || in_y) dEz_dy = dfwd_f<T, R>([&](int d) { return ez_[R + threadIdx.x + d]; }, j, NY);
-      if (dhy || in_x) dEz_dx = dfwd_f<T, R>([&](int d) { return q[R - 1 + d]; }, i, NX);
-      T hx = f.Hx[rb + j], hy = f.Hy[rb + j];
-      if (dhx) hx = hx - cy * dEz_dy;
-      if (dhy) hy = hy + c1 * dEz_dx;
-      if (in_x || in_y) {
-        const T up = f.ch_rhs[c];
-        if (in_x) {
-#pragma unroll
-          for (int fc = 0; fc < 2; ++fc) {
-            const int qq = fc == 0 ? qx0 : qx1;
-            if (qq < 0) continue;
-            const Face<T>& F = a.hF[fc];
-            const Prof<T> pr = prof(F, qq);
-            const long long pi = ((long long)s * F.p + qq) * NY + j;   // (p, NY, 1)
-            const T d = dEz_dx / a.dx, ph = F.psi1[pi];
-            hy += up * (pr.ra1 * d + pr.rb * ph);
-            F.psi1[pi] = pr.re * ph - pr.rf * d;
-          }
-        }
-        if (in_y) {
-#pragma unroll
-          for (int fc = 2; fc < 4; ++fc) {
-            const int qq = fc == 2 ? qy0 : qy1;
-            if (qq < 0) continue;
-            const Face<T>& F = a.hF[fc];
-            const Prof<T> pr = prof(F, qq);
-            const long long pi = ((long long)s * NX + i) * F.p + qq;   // (NX, p, 1)
-            const T d = dEz_dy / a.dy, ph = F.psi1[pi];
-            hx -= up * (pr.ra1 * d + pr.rb * ph);
-            F.psi1[pi] = pr.re * ph - pr.rf * d;
-          }
-        }
-      }
-      f.Hx[rb + j] = hx;
-      f.Hy[rb + j] = hy;
-    }
-#pragma unroll
-    for (int m = 0; m < 2 * R - 1; ++m) q[m] = q[m + 1];
-  }
-}
-
-template <typename T, int R>
-__global__ void __launch_bounds__(T2) k2_fwd_e(TiledFwd<T> P, TmFields<T> f) {
-  constexpr int W = T2 + 2 * R;
-  __shared__ T sHx[2][W];
-  __shared__ float red[33];
-  const FwdArgs<T>& a = P.a;
-  const Grid& g = a.g;
-  const int NX = g.NX, NY = g.NY;
-  const int j0 = blockIdx.x * T2;
-  const int j = j0 + threadIdx.x;
-  const bool colv = j < NY;
-  const int x0 = blockIdx.y * P.xchunk, x1 = min(x0 + P.xchunk, NX);
-  const int s = blockIdx.z;
-  const long long sb = (long long)s * NX * NY;
-  const int it = a.ctrl->cur + a.k_in_chunk;
-  const bool save_r = a.keep_r && (it % a.S == 0);
-  const int slot = it / a.S;
-  const int qy0 = (colv && a.has_cpml && j > 0) ? q_low_e(a.eF[2].p, j) : -1;
-  const int qy1 = (colv && a.has_cpml && j > 0) ? q_high(a.eF[3].p, j, NY) : -1;
-  const int hcol = threadIdx.x < R ? j0 - R + (int)threadIdx.x : j0 + T2 + (int)threadIdx.x - R;
-  const bool hload = threadIdx.x < 2 * R && hcol >= 0 && hcol < NY;
-  const int hs = threadIdx.x < R ? (int)threadIdx.x : T2 + (int)threadIdx.x;
-  T q[2 * R];   // Hy at rows i-R .. i+R-1
-#pragma unroll
-  for (int m = 0; m < 2 * R - 1; ++m) {
-    const int r = x0 - R + m;
-    q[m] = (colv && r >= 0 && r < NX) ? f.Hy[sb + (long long)r * NY + j] : T(0);
-  }
-  for (int i = x0; i < x1; ++i) {
-    const int b = (i - x0) & 1;
-    {
-      const int r = i + R - 1;
-      q[2 * R - 1] = (colv && r < NX) ? f.Hy[sb + (long long)r * NY + j] : T(0);
-    }
-    const long long rb = sb + (long long)i * NY;
-    sHx[b][R + threadIdx.x] = colv ? f.Hx[rb + j] : T(0);
-    if (threadIdx.x < 2 * R) sHx[b][hs] = hload ? f.Hx[rb + hcol] : T(0);
-    __syncthreads();
-    T ez = T(0), oz = T(0), c0e = T(0), cb = T(0);
-    bool dez = false;
-    const int c = i * NY + j;
-    if (colv) {
-      dez = tm_upd_ez(g, i, j);
-      const int qx0 = (a.has_cpml && i > 0) ? q_low_e(a.eF[0].p, i) : -1;
-      const int qx1 = (a.has_cpml && i > 0) ? q_high(a.eF[1].p, i, NX) : -1;
-      const bool in_x = qx0 >= 0 || qx1 >= 0, in_y = qy0 >= 0 || qy1 >= 0;
-      c0e = f.ce_hist[c];
-      const T c1 = f.ce_curl[c];
-      const T cy = curl_scale(c1, a.dx, a.dy, a.dy_eq);
-      oz = ez = f.Ez[rb + j];
-      const T* hx_ = sHx[b];
-      T dHy_dx = T(0), dHx_dy = T(0);
-      if (dez || in_x) dHy_dx = dback_f<T, R>([&](int d) { return q[R + d]; }, i, NX);
-      if (dez || in_y) dHx_dy = dback_f<T, R>([&](int d) { return hx_[R + threadIdx.x + d]; }, j, NY);
-      if (dez) ez = c0e * ez + c1 * dHy_dx - cy * dHx_dy;
-      const int cfull = i * g.sx + j * g.NZ;  // cell index of the full grid (k = 0)
-      const bool src_hit = point_hit(P.src, s, cfull);
-      if (in_x || in_y || src_hit || save_r) cb = f.ce_rhs[c];
-      if (in_x) {
-#pragma unroll
-        for (int fc = 0; fc < 2; ++fc) {
-          const int qq = fc == 0 ? qx0 : qx1;
-          if (qq < 0) continue;
-          const Face<T>& F = a.eF[fc];
-          const Prof<T> pr = prof(F, qq);
-          const long long pi = ((long long)s * (F.p + 1) + qq) * NY + j;   // (p+1, NY, 1)
-          const T d = dHy_dx / a.dx, ph = F.psi2[pi];
-          ez += cb * (pr.ra1 * d + pr.rb * ph);
-          F.psi2[pi] = pr.re * ph - pr.rf * d;
-        }
-      }
-      if (in_y) {
-#pragma unroll
-        for (int fc = 2; fc < 4; ++fc) {
-          const int qq = fc == 2 ? qy0 : qy1;
-          if (qq < 0) continue;
-          const Face<T>& F = a.eF[fc];
-          const Prof<T> pr = prof(F, qq);
-          const long long pi = ((long long)s * NX + i) * (F.p + 1) + qq;  // (NX, p+1, 1)
-          const T d = dHx_dy / a.dy, ph = F.psi2[pi];
-          ez -= cb * (pr.ra1 * d + pr.rb * ph);
-          F.psi2[pi] = pr.re * ph - pr.rf * d;
-        }
-      }
-      if (src_hit) {
-        T ex = T(0), ey = T(0);
-        inject_at(P, s, cfull, it, cb, ex, ey, ez);
-      }
-    }
-    if (save_r) {
-      long long h = 0;
-      const bool inbox = colv && in_box(a.box, i, j, 0, h);
-      T rv = T(0);
-      if (inbox) {
-        const T aeff = dez ? c0e : T(1);
-        rv = cb != T(0) ? (ez - aeff * oz) / cb : T(0);
-      }
-      float inv = 1.0f;
-      if (a.kind == kFP8) {
-        const float am = block_absmax(inbox ? fabsf(float(rv)) : 0.0f, red);
-        const float sc = fp8_scale_of(am);
-        inv = 1.0f / sc;
-        if (threadIdx.x == 0) a.r_scales[((long long)slot * g.nshot + s) * a.ntiles + fp8_tile2(g, i, j0)] = sc;
-      }
-      if (inbox) hist_store<T>(a.R_saved, slot * a.frame + s * a.box.cells() + h, rv, a.kind, inv);
-    }
-    if (colv) {
-      const int cfull = i * g.sx + j * g.NZ;
-      sample_at(P, s, cfull, it, T(0), T(0), ez);
-      f.Ez[rb + j] = ez;
-    }
-#pragma unroll
-    for (int m = 0; m < 2 * R - 1; ++m) q[m] = q[m + 1];
-  }
-}
-
-// (nshot, NX, NY, NZ=2) plane k = 0  <->  compact (nshot, NX, NY).
-template <typename T>
-__global__ void k_pack2d(const T* __restrict__ src, T* __restrict__ dst, long long n) {
-  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < n; w += (long long)gridDim.x * blockDim.x)
-    dst[w] = src[2 * w];
-}
-template <typename T>
-__global__ void k_unpack2d(const T* __restrict__ src, T* __restrict__ dst, long long n) {
-  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < n; w += (long long)gridDim.x * blockDim.x)
-    dst[2 * w] = src[w];
 }
 
 }  // namespace dg

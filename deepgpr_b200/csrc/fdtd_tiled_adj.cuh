@@ -415,220 +415,13 @@ __global__ void __launch_bounds__(256) k3_adj_h(TiledAdj<T> P) {
 }
 
 // ---------------------------------------------------------------------------
-// 2D TM adjoint (compact lambda_Ez, lambda_Hx, lambda_Hy).
-// ---------------------------------------------------------------------------
-template <typename T>
-struct TmAdj {
-  T *lEz, *lHx, *lHy;
-  const T *ce_hist, *ce_curl, *ce_rhs, *ch_curl, *ch_rhs;   // compact (NX, NY)
-};
-
-// E-step channels of the TM fields: B_X (x faces psi2, c lambda_ez) and
-// C_Y (y faces psi2, -c_y lambda_ez).
-template <typename T>
-__device__ __forceinline__ T tm_e_channel(const AdjArgs<T>& a, const TmAdj<T>& t, int ch, int s, int ii, int jj) {
-  const Grid& g = a.g;
-  if (ii < 0 || jj < 0 || ii >= g.NX || jj >= g.NY) return T(0);
-  const int c = ii * g.NY + jj;
-  const long long f = (long long)s * g.NX * g.NY + c;
-  T w = T(0);
-  if (ch == 2) {
-    if (a.has_cpml) add_pml<T, true>(w, a.eF[0], a.eF[1], g, 0, 2, s, ii, jj, 0);
-    if (tm_upd_ez(g, ii, jj)) w += t.ce_curl[c] * t.lEz[f];
-  } else {
-    if (a.has_cpml) add_pml<T, true>(w, a.eF[2], a.eF[3], g, 1, 2, s, ii, jj, 0);
-    if (tm_upd_ez(g, ii, jj)) w += (-scaled(t.ce_curl[c], a.dx, a.dy, a.dy_eq)) * t.lEz[f];
-  }
-  return w;
-}
-
-// H-step channels: A_X (x faces psi1, c lambda_hy), A_Y (y faces psi1, -c_y lambda_hx).
-template <typename T>
-__device__ __forceinline__ T tm_h_channel(const AdjArgs<T>& a, const TmAdj<T>& t, int ch, int s, int ii, int jj) {
-  const Grid& g = a.g;
-  if (ii < 0 || jj < 0 || ii >= g.NX || jj >= g.NY) return T(0);
-  const int c = ii * g.NY + jj;
-  const long long f = (long long)s * g.NX * g.NY + c;
-  T w = T(0);
-  if (ch == 0) {
-    if (a.has_cpml) add_pml<T, false>(w, a.hF[0], a.hF[1], g, 0, 1, s, ii, jj, 0);
-    if (tm_upd_hy(g, ii, jj)) w += t.ch_curl[c] * t.lHy[f];
-  } else {
-    if (a.has_cpml) add_pml<T, false>(w, a.hF[2], a.hF[3], g, 1, 1, s, ii, jj, 0);
-    if (tm_upd_hx(g, ii, jj)) w += (-scaled(t.ch_curl[c], a.dx, a.dy, a.dy_eq)) * t.lHx[f];
-  }
-  return w;
-}
-
-template <typename T, int R>
-__global__ void __launch_bounds__(T2) k2_adj_e(TiledAdj<T> P, TmAdj<T> t) {
-  constexpr int W = T2 + 2 * R;
-  __shared__ T sCY[2][W];
-  const AdjArgs<T>& a = P.a;
-  const Grid& g = a.g;
-  const int NX = g.NX, NY = g.NY;
-  const int it = a.ctrl->cur - a.k_in_chunk;
-  if (a.want_src && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0) {
-    for (int m = threadIdx.x; m < a.nsrc; m += blockDim.x) {
-      T acc = a.grad_source[(long long)m * a.nt + it];
-      for (int s = 0; s < g.nshot; ++s) acc += a.srcv[(long long)s * a.nsrc + m];
-      a.grad_source[(long long)m * a.nt + it] = acc;
-    }
-  }
-  const int j0 = blockIdx.x * T2;
-  const int j = j0 + threadIdx.x;
-  const bool colv = j < NY;
-  const int x0 = blockIdx.y * P.xchunk, x1 = min(x0 + P.xchunk, NX);
-  const int s = blockIdx.z;
-  const long long sb = (long long)s * NX * NY;
-  const int hcol = threadIdx.x < R ? j0 - R + (int)threadIdx.x : j0 + T2 + (int)threadIdx.x - R;
-  const int hs = threadIdx.x < R ? (int)threadIdx.x : T2 + (int)threadIdx.x;
-  const int qy0 = (colv && a.has_cpml) ? q_low_h(a.hF[2].p, j) : -1;
-  const int qy1 = (colv && a.has_cpml) ? q_high(a.hF[3].p, j, NY) : -1;
-  T qB[2 * R];   // B_X at rows i-R+1 .. i+R
-#pragma unroll
-  for (int m = 0; m < 2 * R - 1; ++m) qB[m] = colv ? tm_e_channel(a, t, 2, s, x0 - R + 1 + m, j) : T(0);
-  for (int i = x0; i < x1; ++i) {
-    const int b = (i - x0) & 1;
-    qB[2 * R - 1] = colv ? tm_e_channel(a, t, 2, s, i + R, j) : T(0);
-    sCY[b][R + threadIdx.x] = colv ? tm_e_channel(a, t, 4, s, i, j) : T(0);
-    if (threadIdx.x < 2 * R) sCY[b][hs] = tm_e_channel(a, t, 4, s, i, hcol);
-    __syncthreads();
-    if (colv) {
-      const long long f = sb + (long long)i * NY + j;
-      const T* scy = sCY[b];
-      T hx = t.lHx[f], hy = t.lHy[f];
-      hy += gback<T, R>([&](int d) { return qB[R - 1 + d]; }, i, NX);
-      hx += gback<T, R>([&](int d) { return scy[R + threadIdx.x + d]; }, j, NY);
-      t.lHx[f] = hx;
-      t.lHy[f] = hy;
-      if (a.has_cpml) {
-        const int qx0 = q_low_h(a.hF[0].p, i), qx1 = q_high(a.hF[1].p, i, NX);
-        if (qx0 >= 0 || qx1 >= 0 || qy0 >= 0 || qy1 >= 0) {
-          const T up_h = t.ch_rhs[i * NY + j];
-#pragma unroll
-          for (int fc = 0; fc < 2; ++fc) {
-            const int q = fc == 0 ? qx0 : qx1;
-            if (q < 0) continue;
-            const Face<T>& F = a.hF[fc];
-            const long long pi = ((long long)s * F.p + q) * NY + j;
-            F.w1[pi] = pml_weight(hy, a.inv_dx, up_h, T(1), prof(F, q), &F.psi1[pi]);
-          }
-#pragma unroll
-          for (int fc = 2; fc < 4; ++fc) {
-            const int q = fc == 2 ? qy0 : qy1;
-            if (q < 0) continue;
-            const Face<T>& F = a.hF[fc];
-            const long long pi = ((long long)s * NX + i) * F.p + q;
-            F.w1[pi] = pml_weight(hx, a.inv_dy, up_h, T(-1), prof(F, q), &F.psi1[pi]);
-          }
-        }
-      }
-    }
-#pragma unroll
-    for (int m = 0; m < 2 * R - 1; ++m) qB[m] = qB[m + 1];
-  }
-}
-
-template <typename T, int R, bool PROLOGUE>
-__global__ void __launch_bounds__(T2) k2_adj_h(TiledAdj<T> P, TmAdj<T> t) {
-  constexpr int W = T2 + 2 * R;
-  __shared__ T sAY[2][PROLOGUE ? 1 : W];
-  const AdjArgs<T>& a = P.a;
-  const Grid& g = a.g;
-  const int NX = g.NX, NY = g.NY;
-  const int it = a.ctrl->cur - a.k_in_chunk;
-  const int head = PROLOGUE ? it : it - 1;
-  const int j0 = blockIdx.x * T2;
-  const int j = j0 + threadIdx.x;
-  const bool colv = j < NY;
-  const int x0 = blockIdx.y * P.xchunk, x1 = min(x0 + P.xchunk, NX);
-  const int s = blockIdx.z;
-  const long long sb = (long long)s * NX * NY;
-  const int hcol = threadIdx.x < R ? j0 - R + (int)threadIdx.x : j0 + T2 + (int)threadIdx.x - R;
-  const int hs = threadIdx.x < R ? (int)threadIdx.x : T2 + (int)threadIdx.x;
-  const int qy0 = (colv && a.has_cpml && j > 0) ? q_low_e(a.eF[2].p, j) : -1;
-  const int qy1 = (colv && a.has_cpml && j > 0) ? q_high(a.eF[3].p, j, NY) : -1;
-  T qA[2 * R];   // A_X at rows i-R .. i+R-1
-  if (!PROLOGUE) {
-#pragma unroll
-    for (int m = 0; m < 2 * R - 1; ++m) qA[m] = colv ? tm_h_channel(a, t, 0, s, x0 - R + m, j) : T(0);
-  }
-  for (int i = x0; i < x1; ++i) {
-    const int b = (i - x0) & 1;
-    if (!PROLOGUE) {
-      qA[2 * R - 1] = colv ? tm_h_channel(a, t, 0, s, i + R - 1, j) : T(0);
-      sAY[b][R + threadIdx.x] = colv ? tm_h_channel(a, t, 1, s, i, j) : T(0);
-      if (threadIdx.x < 2 * R) sAY[b][hs] = tm_h_channel(a, t, 1, s, i, hcol);
-      __syncthreads();
-    }
-    if (colv) {
-      const int c = i * NY + j;
-      const long long f = sb + c;
-      T ez = t.lEz[f];
-      if (!PROLOGUE) {
-        if (tm_upd_ez(g, i, j)) ez = t.ce_hist[c] * ez;
-        const T* say = sAY[b];
-        ez += gfwd<T, R>([&](int d) { return qA[R + d]; }, i, NX);
-        ez += gfwd<T, R>([&](int d) { return say[R + threadIdx.x + d]; }, j, NY);
-      }
-      if (head >= 0) {
-        const int cfull = i * g.sx + j * g.NZ;
-        T ex = T(0), ey = T(0);
-        if (point_hit(P.rcv, s, cfull) && a.rx_comp == 2) {
-          const int row = point_row(P.rcv, cfull);
-          for (int e = a.rcv.off[row]; e < a.rcv.off[row + 1]; ++e)
-            if (a.rcv.shot[e] == s) ez += a.data_grad[((long long)s * a.nt + head) * a.nrx + a.rcv.idx[e]];
-        }
-        if (a.want_src && point_hit(P.src, s, cfull)) {
-          const int row = point_row(P.src, cfull);
-          for (int e = a.src.off[row]; e < a.src.off[row + 1]; ++e)
-            if (a.src.shot[e] == s) a.srcv[(long long)s * a.nsrc + a.src.idx[e]] = -t.ce_rhs[c] * a.src_geo * ez;
-        }
-        (void)ex;
-        (void)ey;
-        if (a.has_cpml) {
-          const int qx0 = i > 0 ? q_low_e(a.eF[0].p, i) : -1;
-          const int qx1 = i > 0 ? q_high(a.eF[1].p, i, NX) : -1;
-          if (qx0 >= 0 || qx1 >= 0 || qy0 >= 0 || qy1 >= 0) {
-            const T up_e = t.ce_rhs[c];
-#pragma unroll
-            for (int fc = 0; fc < 2; ++fc) {
-              const int q = fc == 0 ? qx0 : qx1;
-              if (q < 0) continue;
-              const Face<T>& F = a.eF[fc];
-              const long long pi = ((long long)s * (F.p + 1) + q) * NY + j;
-              F.w2[pi] = pml_weight(ez, a.inv_dx, up_e, T(1), prof(F, q), &F.psi2[pi]);
-            }
-#pragma unroll
-            for (int fc = 2; fc < 4; ++fc) {
-              const int q = fc == 2 ? qy0 : qy1;
-              if (q < 0) continue;
-              const Face<T>& F = a.eF[fc];
-              const long long pi = ((long long)s * NX + i) * (F.p + 1) + q;
-              F.w2[pi] = pml_weight(ez, a.inv_dy, up_e, T(-1), prof(F, q), &F.psi2[pi]);
-            }
-          }
-        }
-      }
-      t.lEz[f] = ez;
-    }
-    if (!PROLOGUE) {
-#pragma unroll
-      for (int m = 0; m < 2 * R - 1; ++m) qA[m] = qA[m + 1];
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------
 // Imaging condition of one saved step (deepgpr_cpu.c:1659-1745).
 // One thread per history-box cell; shots and components summed inside the
 // thread in the reference's order.  lam_* point at lambda_E before the
-// ce_hist scaling of this step.  tm2d: lambda_ez is compact (shot, NX, NY).
+// ce_hist scaling of this step.  3D grids (the 2D TM path uses tm_image).
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(256) k_image(AdjArgs<T> a, const T* lam_x, const T* lam_y, const T* lam_z,
-                                               int tm2d) {
+__global__ void __launch_bounds__(256) k_image(AdjArgs<T> a, const T* lam_x, const T* lam_y, const T* lam_z) {
   const Grid& g = a.g;
   const int it = a.ctrl->cur - a.k_in_chunk;
   if (it % a.S != 0) return;
@@ -640,8 +433,8 @@ __global__ void __launch_bounds__(256) k_image(AdjArgs<T> a, const T* lam_x, con
   const int rem = int(hidx % ((long long)a.box.ny * a.box.nz));
   const int i = hi + a.box.x0, j = rem / a.box.nz + a.box.y0, k = rem % a.box.nz + a.box.z0;
   const int c = i * g.sx + j * g.NZ + k;
-  const int cl = tm2d ? i * g.NY + j : c;           // index into lambda arrays
-  const long long lcells = tm2d ? (long long)g.NX * g.NY : g.cells;
+  const int cl = c;
+  const long long lcells = g.cells;
   const T ca = a.ce_hist[c], cbv = a.ce_rhs[c];
   int w = a.S;
   if (it + w > a.nt) w = a.nt - it;
@@ -653,7 +446,7 @@ __global__ void __launch_bounds__(256) k_image(AdjArgs<T> a, const T* lam_x, con
   const T dcb_s = T(-0.5) * cbv * cbv;
   const bool dex = upd_ex(g, i, j, k), dey = upd_ey(g, i, j, k), dez = upd_ez(g, i, j, k);
   const int ncomp = a.mode == 3 ? 3 : 1;
-  const long long tile = tm2d ? fp8_tile2(g, i, j) : fp8_tile3(g, i, j, k);
+  const long long tile = fp8_tile3(g, i, j, k);
   T loc_e = T(0), loc_s = T(0);
   double loc_e64 = 0.0, loc_s64 = 0.0;
   for (int s = 0; s < g.nshot; ++s) {

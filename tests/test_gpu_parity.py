@@ -153,3 +153,30 @@ def test_fp8_history_gradient(dims, cuda_device, oracle_lib):
     assert rel_l2(got["receivers"], ref["receivers"]) <= RX_TOL
     assert rel_l2(got["grad_eps"], ref["grad_eps"]) < 5e-2
     assert rel_l2(got["grad_sigma"], ref["grad_sigma"]) < 5e-2
+
+
+@pytest.mark.parametrize("order", [2, 4, 8])
+def test_2d_wide_grid_interior_fast_paths(order, cuda_device, oracle_lib):
+    """NY = 321 field columns: the middle 128-column warp segments take the interior fast paths."""
+    p = problem_2d(nt=90, order=order, shape=(60, 300), want_source=True)
+    p.source_location = torch.tensor([[[30, 150, 0]], [[20, 40, 0]]], dtype=torch.int32)
+    p.receiver_location = torch.tensor([[[10, j, 0] for j in range(0, 300, 25)]] * 2, dtype=torch.int32)
+    ref = driver.run(p, "oracle")
+    got = run_product(p, cuda_device)
+    _compare(got, ref, grads=("grad_eps", "grad_sigma", "grad_source"))
+
+
+@pytest.mark.parametrize("kind", [2, 1])
+def test_2d_wide_grid_stored_rhs(kind, cuda_device, oracle_lib):
+    p = problem_2d(nt=80, order=4, shape=(50, 280), storage_kind=kind, rhs_from_e=False)
+    ref = driver.run(p, "oracle")
+    got = run_product(p, cuda_device)
+    _compare(got, ref)
+
+
+def test_2d_wide_grid_fp8(cuda_device, oracle_lib):
+    p = problem_2d(nt=120, order=4, shape=(50, 280))
+    ref = driver.run(p, "oracle")
+    got = run_product(p, cuda_device, wavefield_compression="fp8")
+    assert rel_l2(got["receivers"], ref["receivers"]) <= RX_TOL
+    assert rel_l2(got["grad_eps"], ref["grad_eps"]) < 5e-2
