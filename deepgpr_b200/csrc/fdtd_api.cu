@@ -174,9 +174,75 @@ struct Scratch {
   }
 };
 
+// ---------------------------------------------------------------------------
+// Static device scratch of dgb_forward_noalloc.  Some callers cannot let a
+// solve allocate device memory: a serving process that has handed the free
+// memory of the GPU to its own pool (an allocation would fail or force the
+// pool to trim), or code that owns a fixed per-request memory budget.  For
+// them the forward solve takes its scratch (control block, source / receiver
+// tables and bitmaps, the pitched 2D working copy) from this file-scope array
+// instead of cudaMallocAsync.  A call whose scratch does not fit is rejected
+// with an error before any time step runs.  Every byte a call uses is written
+// by that call before it is read (tables and bitmaps are uploaded whole, the
+// control block is set by k_set, the pitched copy is written by the pack
+// kernels including its zero padding), so nothing needs clearing between
+// calls.  All calls on a device share the array: overlapping calls (from two
+// threads, or on two streams) race.
+// ---------------------------------------------------------------------------
+constexpr size_t kNoAllocScratchBytes = size_t(8) << 20;   // 8 MiB per device
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+// Address of the static scratch on the current device, looked up once per
+// device (the first dgb_forward_noalloc call on a device does this set-up).
+char* noalloc_scratch_base() {
+  static std::mutex mu;
+  static char* base[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    set_error("dgb_forward_noalloc: no usable current CUDA device");
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lock(mu);
+  if (!base[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) {
+      set_error("dgb_forward_noalloc: cudaGetSymbolAddress of the static scratch failed: %s", cudaGetErrorString(e));
+      return nullptr;
+    }
+    base[dev] = static_cast<char*>(p);
+  }
+  return base[dev];
+}
+
+// Bump allocator over the static scratch, with the interface of Scratch.
+struct StaticScratch {
+  cudaStream_t st;
+  char* base;
+  size_t used = 0;
+  bool failed = false;
+  explicit StaticScratch(cudaStream_t s) : st(s), base(noalloc_scratch_base()) { failed = base == nullptr; }
+  template <typename P>
+  P* get(size_t bytes) {
+    if (failed) return nullptr;
+    if (bytes == 0) bytes = 16;
+    const size_t off = (used + 255) & ~size_t(255);
+    if (off + bytes > kNoAllocScratchBytes) {
+      set_error("dgb_forward_noalloc: this solve needs more than the %zu bytes of static device scratch "
+                "(%zu requested at offset %zu); use forward for it",
+                kNoAllocScratchBytes, bytes, off);
+      failed = true;
+      return nullptr;
+    }
+    used = off + bytes;
+    return reinterpret_cast<P*>(base + off);
+  }
+};
+
 // Sorted point table (see PointTable in fdtd_common.cuh) built on the host
 // from the caller's (nshot, npts, 3) int32 locations.
-bool build_table(const int* loc, int nshot, int npts, const Grid& g, cudaStream_t st, Scratch& scratch,
+template <typename Alloc>
+bool build_table(const int* loc, int nshot, int npts, const Grid& g, cudaStream_t st, Alloc& scratch,
                  PointTable* out, const char* what, int err_code) {
   out->n = 0;
   out->cells = out->off = out->shot = out->idx = nullptr;
@@ -222,7 +288,7 @@ bool build_table(const int* loc, int nshot, int npts, const Grid& g, cudaStream_
   packed.insert(packed.end(), off.begin(), off.end());
   packed.insert(packed.end(), shot.begin(), shot.end());
   packed.insert(packed.end(), idx.begin(), idx.end());
-  int* d = scratch.get<int>(packed.size() * sizeof(int));
+  int* d = scratch.template get<int>(packed.size() * sizeof(int));
   if (!d) return false;
   if (!cuda_ok(cudaMemcpyAsync(d, packed.data(), packed.size() * sizeof(int), cudaMemcpyHostToDevice, st), what))
     return false;
@@ -237,7 +303,8 @@ bool build_table(const int* loc, int nshot, int npts, const Grid& g, cudaStream_
 }
 
 // Table plus per-shot membership bitmaps.
-bool build_pointset(const int* loc, int nshot, int npts, const Grid& g, cudaStream_t st, Scratch& scratch,
+template <typename Alloc>
+bool build_pointset(const int* loc, int nshot, int npts, const Grid& g, cudaStream_t st, Alloc& scratch,
                     PointSet* ps, PointTable* tb_out, const char* what, int err_code,
                     const unsigned char** rows_out = nullptr, std::vector<char>* any_rows = nullptr) {
   if (rows_out) *rows_out = nullptr;
@@ -260,7 +327,7 @@ bool build_pointset(const int* loc, int nshot, int npts, const Grid& g, cudaStre
       const int c = p[0] * g.sx + p[1] * g.NZ + p[2];
       bits[(size_t)s * ps->words_per_shot + (c >> 5)] |= 1u << (c & 31);
     }
-  unsigned* d = scratch.get<unsigned>(bits.size() * sizeof(unsigned));
+  unsigned* d = scratch.template get<unsigned>(bits.size() * sizeof(unsigned));
   if (!d) return false;
   if (!cuda_ok(cudaMemcpyAsync(d, bits.data(), bits.size() * sizeof(unsigned), cudaMemcpyHostToDevice, st), what))
     return false;
@@ -274,7 +341,7 @@ bool build_pointset(const int* loc, int nshot, int npts, const Grid& g, cudaStre
     std::vector<unsigned char> rows((size_t)nshot * g.NX, 0);
     for (int s = 0; s < nshot; ++s)
       for (int m = 0; m < npts; ++m) rows[(size_t)s * g.NX + h[((size_t)s * npts + m) * 3]] = 1;
-    unsigned char* dr = scratch.get<unsigned char>(rows.size());
+    unsigned char* dr = scratch.template get<unsigned char>(rows.size());
     if (!dr) return false;
     if (!cuda_ok(cudaMemcpyAsync(dr, rows.data(), rows.size(), cudaMemcpyHostToDevice, st), what)) return false;
     if (!cuda_ok(cudaStreamSynchronize(st), what)) return false;
@@ -638,7 +705,7 @@ struct ForwardCall {
   int save_model_history;
 };
 
-template <typename T>
+template <typename T, typename Alloc = Scratch>
 void forward_impl(const ForwardCall<T>& fc) {
   g_error[0] = '\0';
   const Common<T>& cm = fc.cm;
@@ -698,7 +765,7 @@ void forward_impl(const ForwardCall<T>& fc) {
     return;
   bool ok = true;
   {
-    Scratch scratch(st);
+    Alloc scratch(st);
     TiledFwd<T> P;
     memset(&P, 0, sizeof(P));
     FwdArgs<T>& a = P.a;
@@ -744,7 +811,7 @@ void forward_impl(const ForwardCall<T>& fc) {
       a.e_scales = reinterpret_cast<float*>(static_cast<char*>(fc.E_saved) + fp8_payload_bytes(vals));
       if (keep_r) a.r_scales = reinterpret_cast<float*>(static_cast<char*>(fc.R_saved) + fp8_payload_bytes(vals));
     }
-    Control* ctrl = scratch.get<Control>(sizeof(Control));
+    Control* ctrl = scratch.template get<Control>(sizeof(Control));
     ok = !scratch.failed;
     const int R = radius_of(g_opt.order_override ? g_opt.order_override : g_order);
     TmGeom tg;
@@ -767,7 +834,7 @@ void forward_impl(const ForwardCall<T>& fc) {
     memset(&tf, 0, sizeof(tf));
     const long long plane2 = (long long)g.NX * tg.NYP;
     if (ok && tm2d) {
-      T* buf = scratch.get<T>((size_t)(3 * g.nshot + 5) * plane2 * sizeof(T));
+      T* buf = scratch.template get<T>((size_t)(3 * g.nshot + 5) * plane2 * sizeof(T));
       ok = buf != nullptr;
       if (ok) {
         tf.Ez = buf;
@@ -1332,6 +1399,40 @@ static void forward_entry(ForwardCall<T>& fc) {
   backward_impl<T>(bc)
 
 DGB_API void forward(DGB_FWD_PARAMS(float)) { DGB_FORWARD_BODY(float); }
+
+// forward() without device memory allocation: its scratch comes from the
+// static array g_noalloc_scratch (8 MiB per device) and its time-step
+// kernels are launched one by one.  See StaticScratch for the callers this
+// serves, the size limit and why overlapping calls race.  The first call on
+// a device does set-up (the scratch address lookup; on a new thread also the
+// library's stream and events): make it before any stream capture.
+template <typename T>
+static void forward_noalloc_entry(ForwardCall<T>& fc) {
+  const int saved = g_opt.use_graph;
+  g_opt.use_graph = 0;
+  forward_impl<T, StaticScratch>(fc);
+  g_opt.use_graph = saved;
+}
+
+DGB_API void dgb_forward_noalloc(DGB_FWD_PARAMS(float)) {
+  ForwardCall<float> fc;
+  memset(&fc, 0, sizeof(fc));
+  DGB_FILL_COMMON(fc.cm);
+  float* ep[12] = {x0e1, x0e2, xme1, xme2, y0e1, y0e2, yme1, yme2, z0e1, z0e2, zme1, zme2};
+  float* hp[12] = {x0h1, x0h2, xmh1, xmh2, y0h1, y0h2, ymh1, ymh2, z0h1, z0h2, zmh1, zmh2};
+  for (int q = 0; q < 12; ++q) {
+    fc.cm.ePsi[q] = ep[q];
+    fc.cm.hPsi[q] = hp[q];
+  }
+  fc.E_saved = E_saved;
+  fc.R_saved = R_saved;
+  fc.Ex = Ex; fc.Ey = Ey; fc.Ez = Ez; fc.Hx = Hx; fc.Hy = Hy; fc.Hz = Hz;
+  fc.nrx = nrx; fc.rx_loc = rx_loc; fc.rx = rx_out; fc.rx_comp = rx_comp;
+  fc.nsrc = nsrc; fc.src_loc = src_loc; fc.wave = src_wave; fc.src_comp = src_comp;
+  fc.save_model_history = save_model_history;
+  (void)use_async_offload;
+  forward_noalloc_entry<float>(fc);
+}
 DGB_API void backward(DGB_BWD_PARAMS(float)) { DGB_BACKWARD_BODY(float); }
 DGB_API void dgb_forward_f64(DGB_FWD_PARAMS(double)) { DGB_FORWARD_BODY(double); }
 DGB_API void dgb_backward_f64(DGB_BWD_PARAMS(double)) { DGB_BACKWARD_BODY(double); }

@@ -134,6 +134,7 @@ SOLVER_SYMBOLS = {
     "backward": (BACKWARD_SIGNATURE, "float"),
     "dgb_forward_f64": (FORWARD_SIGNATURE, "double"),
     "dgb_backward_f64": (BACKWARD_SIGNATURE, "double"),
+    "dgb_forward_noalloc": (FORWARD_SIGNATURE, "float"),
 }
 
 _CT = {

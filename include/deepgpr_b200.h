@@ -138,6 +138,42 @@ long long dgb_history_bytes(int kind, int ncomp, int nt_saved, int nshot, long l
 void dgb_forward_f64(/* forward's parameters, float -> double */);
 void dgb_backward_f64(/* backward's parameters, float -> double */);
 
+/* No counterpart in the reference.  forward() without device memory
+ * allocation, for callers that cannot allocate during a solve: a serving
+ * process whose free GPU memory belongs to its own pool (an allocation would
+ * fail or make the pool trim), or code holding a fixed per-request memory
+ * budget.  Same parameters, results and errors as forward().  Its device
+ * scratch (control block, source / receiver tables and bitmaps, the pitched
+ * 2D working copy) is a static array of DGB_NOALLOC_SCRATCH_BYTES (8 MiB) per
+ * device; a solve whose scratch does not fit is rejected through
+ * deepgpr_last_error() before any time step runs.  The first call on a device
+ * does set-up (it looks up the array's address; on a new thread it also
+ * creates the library's stream and events): make it before any stream
+ * capture.  All calls on a device share the array, so overlapping calls (two
+ * threads, or two streams) race. */
+#define DGB_NOALLOC_SCRATCH_BYTES 8388608
+void dgb_forward_noalloc(
+    const float* eps_r_pad, const float* sigma_pad, const float* mu_r_pad,
+    void* E_saved, void* R_saved,
+    float* Ex, float* Ey, float* Ez, float* Hx, float* Hy, float* Hz,
+    float* ce_hist, float* ce_curl, float* ce_rhs, float* ch_hist, float* ch_curl, float* ch_rhs,
+    float* x0_e_phi1, float* x0_e_phi2, float* x0_h_phi1, float* x0_h_phi2,
+    float* xm_e_phi1, float* xm_e_phi2, float* xm_h_phi1, float* xm_h_phi2,
+    float* y0_e_phi1, float* y0_e_phi2, float* y0_h_phi1, float* y0_h_phi2,
+    float* ym_e_phi1, float* ym_e_phi2, float* ym_h_phi1, float* ym_h_phi2,
+    float* z0_e_phi1, float* z0_e_phi2, float* z0_h_phi1, float* z0_h_phi2,
+    float* zm_e_phi1, float* zm_e_phi2, float* zm_h_phi1, float* zm_h_phi2,
+    int pml_x0, int pml_xm, int pml_y0, int pml_ym, int pml_z0, int pml_zm,
+    const float* x0_e_coeff, const float* xm_e_coeff, const float* y0_e_coeff,
+    const float* ym_e_coeff, const float* z0_e_coeff, const float* zm_e_coeff,
+    const float* x0_h_coeff, const float* xm_h_coeff, const float* y0_h_coeff,
+    const float* ym_h_coeff, const float* z0_h_coeff, const float* zm_h_coeff,
+    float dt, int nt, int nshot, int nreceiver, float dx, float dy, float dz,
+    const int* receiver_location, float* receiver_data, int receiver_component,
+    int nx_fields, int ny_fields, int nz_fields, int nsource,
+    const int* source_location, const float* source_waveform, int source_component,
+    int sampling_interval, int fwi_mode, int storage_type, int save_model_history, int use_async_offload);
+
 /* Process-wide kernel timing (CUDA events around every time-step
  * kernel; graph replay is off while enabled).  dgb_profile(1) clears the
  * totals; dgb_profile_read fills ms[k] and launches[k] for the kinds

@@ -48,6 +48,7 @@ def test_python_tables_match_header():
     assert [n for n, _ in native.BACKWARD_SIGNATURE] == _params("backward")
     assert len(native.FORWARD_SIGNATURE) == 81
     assert len(native.BACKWARD_SIGNATURE) == 86
+    assert _params("dgb_forward_noalloc") == _params("forward")
 
 
 def test_header_matches_reference_parameter_order():
