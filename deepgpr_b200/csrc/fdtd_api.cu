@@ -352,6 +352,9 @@ bool build_pointset(const int* loc, int nshot, int npts, const Grid& g, cudaStre
   return true;
 }
 
+// Elements past the last plane of the 2D TM working copy (see tm_plan).
+constexpr size_t kTmTailPad = 4 * TMW + 64;
+
 // Strip layout of the 2D TM path: padded pitch and 32-column strips; the
 // rectangles and row chunking of each launch are set by tm_plan.
 TmGeom tm_layout(const Grid& g) {
@@ -380,9 +383,11 @@ int blocks_per_sm(K kernel) {
 
 // Appends rectangle (warp strips of `width` columns starting at column
 // 32 * seg0, nseg of them; rows [row0, row1)) with chunks of xc rows.
-void tm_add_rect(TmGeom& tg, int nshot, int seg0, int nseg, int width, int row0, int row1, int xc) {
-  if (nseg <= 0 || row1 <= row0) return;
+void tm_add_rect(TmGeom& tg, int nshot, int seg0, int nseg, int width, int row0, int row1, int xc,
+                 int kind = kFrameGeneral) {
+  if (nseg <= 0 || row1 <= row0 || tg.nrect >= kTmMaxRects) return;
   TmRect& r = tg.rect[tg.nrect++];
+  r.kind = kind;
   r.seg0 = seg0;
   r.nseg = nseg;
   r.width = width;
@@ -395,13 +400,16 @@ void tm_add_rect(TmGeom& tg, int nshot, int seg0, int nseg, int width, int row0,
 }
 
 // Interior rectangle of one 2D TM half step and the frame of general work
-// around it.  Interior rows: the longest run where tm_lean_ok holds; interior
-// columns: the longest run of whole 32-column tiles where it holds (so each
+// around it.  Interior rows: runs where tm_lean_ok holds along x and no shot
+// has a source or receiver (at most 4, the longest); interior columns: the
+// longest run of whole 32-column tiles where tm_lean_ok holds along y (so each
 // FP8 scale tile is written by one kernel).  The interior kernels use
-// 64-column strips starting at the first interior column, chunked so a launch
-// is about one wave of resident warps (occupancy `iblocks` CTAs per SM,
-// chunks of at least 16 rows); the frame (32-column strips) uses 8-row chunks,
-// its work being latency-bound.
+// 128-column strips from the first interior column (tiles past the interior
+// are masked), chunked so a launch is about one wave of resident warps
+// (occupancy `iblocks` CTAs per SM, chunks of at least 16 rows).  The frame
+// is split by kind (see kFrameGeneral): edge tiles on x-lean rows, edge tiles
+// elsewhere (corners, chunks of 2 rows), and interior tiles on the remaining
+// rows (chunks of 8 rows), all in one launch.
 struct TmPlan {
   TmGeom interior, frame;
 };
@@ -411,89 +419,110 @@ TmPlan tm_plan(const TmGeom& base, const Grid& g, int kind, int R, const TmFaces
   TmPlan pl;
   pl.interior = base;
   pl.frame = base;
-  // interior row runs: tm_lean_ok rows that hold no source / receiver of any shot
-  std::vector<std::pair<int, int>> runs;
+  // the interior kernels index a shot plane with 32-bit offsets
+  if ((long long)g.NX * base.NYP + (long long)kTmTailPad >= (1LL << 31)) lean = false;
+  auto runs_of = [](int n, auto ok) {
+    std::vector<std::pair<int, int>> r;
+    int cur = -1;
+    for (int c = 0; c <= n; ++c) {
+      const bool y = c < n && ok(c);
+      if (y && cur < 0) cur = c;
+      if (!y && cur >= 0) {
+        r.push_back({cur, c});
+        cur = -1;
+      }
+    }
+    return r;
+  };
+  auto complement = [](int n, const std::vector<std::pair<int, int>>& in) {
+    std::vector<std::pair<int, int>> r;
+    int prev = 0;
+    for (auto& q : in) {
+      if (q.first > prev) r.push_back({prev, q.first});
+      prev = q.second;
+    }
+    if (n > prev) r.push_back({prev, n});
+    return r;
+  };
+  std::vector<std::pair<int, int>> xl, rows;
   int tlo = 0, thi = 0;
   if (lean) {
-    int cur = -1;
-    for (int i = 0; i <= g.NX; ++i) {
-      const bool y = i < g.NX && tm_lean_ok(kind, 0, i, g.NX, R, f) && !(avoid && !avoid->empty() && (*avoid)[i]);
-      if (y && cur < 0) cur = i;
-      if (!y && cur >= 0) {
-        runs.push_back({cur, i});
-        cur = -1;
+    xl = runs_of(g.NX, [&](int i) { return tm_lean_ok(kind, 0, i, g.NX, R, f); });
+    rows = runs_of(g.NX, [&](int i) {
+      return tm_lean_ok(kind, 0, i, g.NX, R, f) && !(avoid && !avoid->empty() && (*avoid)[i]);
+    });
+    if (rows.size() > 4) {
+      std::sort(rows.begin(), rows.end(), [](const std::pair<int, int>& x, const std::pair<int, int>& y) {
+        return x.second - x.first > y.second - y.first;
+      });
+      rows.resize(4);
+      std::sort(rows.begin(), rows.end());
+    }
+    const auto tiles = runs_of(base.nseg, [&](int q) {
+      for (int j = q * TMW; j < (q + 1) * TMW; ++j)
+        if (!tm_lean_ok(kind, 1, j, g.NY, R, f)) return false;
+      return true;
+    });
+    for (auto& t : tiles)
+      if (t.second - t.first > thi - tlo) {
+        tlo = t.first;
+        thi = t.second;
       }
-    }
-    // at most 4 interior runs (the longest), kept in row order
-    if (runs.size() > 4) {
-      std::sort(runs.begin(), runs.end(),
-                [](const std::pair<int, int>& x, const std::pair<int, int>& y) { return x.second - x.first > y.second - y.first; });
-      runs.resize(4);
-      std::sort(runs.begin(), runs.end());
-    }
-    cur = -1;
-    for (int q = 0; q <= base.nseg; ++q) {
-      bool y = q < base.nseg;
-      for (int j = q * TMW; y && j < (q + 1) * TMW; ++j) y = tm_lean_ok(kind, 1, j, g.NY, R, f);
-      if (y && cur < 0) cur = q;
-      if (!y && cur >= 0) {
-        if (q - cur > thi - tlo) {
-          tlo = cur;
-          thi = q;
-        }
-        cur = -1;
-      }
-    }
   }
-  const int frame_xc = 8;
-  if (!runs.empty() && thi > tlo) {
-    const int n64 = (thi - tlo + 1) / 2;
-    int rows = 0;
-    for (auto& r : runs) rows += r.second - r.first;
-    const long long per = (long long)n64 * g.nshot;
+  const auto xg = complement(g.NX, xl);
+  const auto mid = complement(g.NX, rows);
+  const bool fits = 2 * xl.size() + 2 * xg.size() + mid.size() <= (size_t)kTmMaxRects;
+  const int frame_xc = 8, corner_xc = 2;
+  if (!rows.empty() && thi > tlo && fits) {
+    const int n128 = (thi - tlo + 3) / 4;
+    int nrows = 0;
+    for (auto& r : rows) nrows += r.second - r.first;
+    const long long per = (long long)n128 * g.nshot;
     const long long resident = (long long)sm_count() * iblocks * TM_WARPS;
     long long chunks = std::max<long long>(1, resident / per);
-    chunks = std::min<long long>(chunks, std::max(1, rows / 16));
-    const int xc = (int)((rows + chunks - 1) / chunks);
-    for (auto& r : runs) tm_add_rect(pl.interior, g.nshot, tlo, n64, 2 * TMW, r.first, r.second, xc);
+    chunks = std::min<long long>(chunks, std::max(1, nrows / 16));
+    const int xc = (int)((nrows + chunks - 1) / chunks);
+    for (auto& r : rows) tm_add_rect(pl.interior, g.nshot, tlo, n128, 4 * TMW, r.first, r.second, xc);
     pl.interior.col1 = thi * TMW;
-    tm_add_rect(pl.frame, g.nshot, 0, tlo, TMW, 0, g.NX, frame_xc);
-    tm_add_rect(pl.frame, g.nshot, thi, base.nseg - thi, TMW, 0, g.NX, frame_xc);
-    int prev = 0;
-    for (auto& r : runs) {
-      tm_add_rect(pl.frame, g.nshot, tlo, thi - tlo, TMW, prev, r.first, frame_xc);
-      prev = r.second;
+    for (auto& r : xl) {
+      tm_add_rect(pl.frame, g.nshot, 0, tlo, TMW, r.first, r.second, frame_xc, kFrameXLean);
+      tm_add_rect(pl.frame, g.nshot, thi, base.nseg - thi, TMW, r.first, r.second, frame_xc, kFrameXLean);
     }
-    tm_add_rect(pl.frame, g.nshot, tlo, thi - tlo, TMW, prev, g.NX, frame_xc);
+    for (auto& r : xg) {
+      tm_add_rect(pl.frame, g.nshot, 0, tlo, TMW, r.first, r.second, corner_xc, kFrameGeneral);
+      tm_add_rect(pl.frame, g.nshot, thi, base.nseg - thi, TMW, r.first, r.second, corner_xc, kFrameGeneral);
+    }
+    for (auto& r : mid) tm_add_rect(pl.frame, g.nshot, tlo, thi - tlo, TMW, r.first, r.second, frame_xc, kFrameYLean);
   } else {
-    tm_add_rect(pl.frame, g.nshot, 0, base.nseg, TMW, 0, g.NX, frame_xc);
+    tm_add_rect(pl.frame, g.nshot, 0, base.nseg, TMW, 0, g.NX, frame_xc, kFrameGeneral);
   }
   return pl;
 }
 
 // 2D imaging kernel for the call's history format.
 template <typename T, int KIND>
-void launch_tm_image_k(bool e_only, bool acc64, unsigned blocks, cudaStream_t st, const AdjArgs<T>& a, const T* lam,
-                       const TmGeom& tg) {
+void launch_tm_image_k(bool e_only, bool acc64, cudaStream_t st, const AdjArgs<T>& a, const T* lam, const TmGeom& tg) {
+  const unsigned blocks = (unsigned)((a.box.cells() + kImageThreads - 1) / kImageThreads);
+  constexpr int B = kImageThreads;
   if (e_only) {
-    if (acc64) tm_image<T, KIND, true, true><<<blocks, 256, 0, st>>>(a, lam, tg.NYP, tg.nseg);
-    else tm_image<T, KIND, true, false><<<blocks, 256, 0, st>>>(a, lam, tg.NYP, tg.nseg);
+    if (acc64) tm_image<T, KIND, true, true><<<blocks, B, 0, st>>>(a, lam, tg.NYP, tg.nseg);
+    else tm_image<T, KIND, true, false><<<blocks, B, 0, st>>>(a, lam, tg.NYP, tg.nseg);
   } else {
-    if (acc64) tm_image<T, KIND, false, true><<<blocks, 256, 0, st>>>(a, lam, tg.NYP, tg.nseg);
-    else tm_image<T, KIND, false, false><<<blocks, 256, 0, st>>>(a, lam, tg.NYP, tg.nseg);
+    if (acc64) tm_image<T, KIND, false, true><<<blocks, B, 0, st>>>(a, lam, tg.NYP, tg.nseg);
+    else tm_image<T, KIND, false, false><<<blocks, B, 0, st>>>(a, lam, tg.NYP, tg.nseg);
   }
 }
 
 template <typename T>
-void launch_tm_image(int kind, bool e_only, bool acc64, unsigned blocks, cudaStream_t st, const AdjArgs<T>& a,
-                     const T* lam, const TmGeom& tg) {
+void launch_tm_image(int kind, bool e_only, bool acc64, cudaStream_t st, const AdjArgs<T>& a, const T* lam,
+                     const TmGeom& tg) {
   if constexpr (sizeof(T) == 8) {
-    launch_tm_image_k<T, kF64>(e_only, acc64, blocks, st, a, lam, tg);
+    launch_tm_image_k<T, kF64>(e_only, acc64, st, a, lam, tg);
   } else {
-    if (kind == kF16) launch_tm_image_k<T, kF16>(e_only, acc64, blocks, st, a, lam, tg);
-    else if (kind == kBF16) launch_tm_image_k<T, kBF16>(e_only, acc64, blocks, st, a, lam, tg);
-    else if (kind == kFP8) launch_tm_image_k<T, kFP8>(e_only, acc64, blocks, st, a, lam, tg);
-    else launch_tm_image_k<T, kF32>(e_only, acc64, blocks, st, a, lam, tg);
+    if (kind == kF16) launch_tm_image_k<T, kF16>(e_only, acc64, st, a, lam, tg);
+    else if (kind == kBF16) launch_tm_image_k<T, kBF16>(e_only, acc64, st, a, lam, tg);
+    else if (kind == kFP8) launch_tm_image_k<T, kFP8>(e_only, acc64, st, a, lam, tg);
+    else launch_tm_image_k<T, kF32>(e_only, acc64, st, a, lam, tg);
   }
 }
 
@@ -501,20 +530,23 @@ void launch_tm_image(int kind, bool e_only, bool acc64, unsigned blocks, cudaStr
 // joined back to st, beside the interior kernel on st.  Returns the number
 // of kernels launched.
 template <typename FrameFn, typename InteriorFn>
-int split_launch(cudaStream_t st, const StreamSet* ss, bool has_interior, FrameFn frame, InteriorFn interior) {
+int split_launch(cudaStream_t st, const StreamSet* ss, const TmPlan& pl, FrameFn frame, InteriorFn interior) {
+  const bool has_interior = pl.interior.nwarps > 0;
   if (!has_interior || ss == nullptr || ss->side == nullptr) {
-    frame(st);
+    frame(st, pl.frame);
     if (has_interior) interior(st);
     return has_interior ? 2 : 1;
   }
   cudaEventRecord(ss->fork, st);
   cudaStreamWaitEvent(ss->side, ss->fork, 0);
-  frame(ss->side);
+  frame(ss->side, pl.frame);
   cudaEventRecord(ss->join, ss->side);
   interior(st);
   cudaStreamWaitEvent(st, ss->join, 0);
   return 2;
 }
+
+dim3 tm_grid(const TmGeom& tg) { return dim3((unsigned)std::max<long long>(1, (tg.nwarps + TM_WARPS - 1) / TM_WARPS)); }
 
 template <typename T>
 TmFaces tm_faces(const Face<T>* eF, const Face<T>* hF, bool cpml) {
@@ -527,7 +559,6 @@ TmFaces tm_faces(const Face<T>* eF, const Face<T>* hF, bool cpml) {
   return f;
 }
 
-dim3 tm_grid(const TmGeom& tg) { return dim3((unsigned)std::max<long long>(1, (tg.nwarps + TM_WARPS - 1) / TM_WARPS)); }
 
 // x-chunk length that gives about 8 resident CTAs per SM.
 int pick_xchunk(int NX, long long tiles_per_plane, int nshot, int min_chunk) {
@@ -834,7 +865,10 @@ void forward_impl(const ForwardCall<T>& fc) {
     memset(&tf, 0, sizeof(tf));
     const long long plane2 = (long long)g.NX * tg.NYP;
     if (ok && tm2d) {
-      T* buf = scratch.template get<T>((size_t)(3 * g.nshot + 5) * plane2 * sizeof(T));
+      // + two y-scaled curl planes when dy != dx, + a tail pad: masked lanes of the
+      // last interior strip may read up to 4 * 32 columns past a row end
+      const int ncoef = cm.dy == cm.dx ? 5 : 7;
+      T* buf = scratch.template get<T>(((size_t)(3 * g.nshot + ncoef) * plane2 + kTmTailPad) * sizeof(T));
       ok = buf != nullptr;
       if (ok) {
         tf.Ez = buf;
@@ -848,6 +882,15 @@ void forward_impl(const ForwardCall<T>& fc) {
         tf.ce_rhs = cf + 2 * plane2;
         tf.ch_curl = cf + 3 * plane2;
         tf.ch_rhs = cf + 4 * plane2;
+        tf.ce_curl_y = tf.ce_curl;
+        tf.ch_curl_y = tf.ch_curl;
+        if (ncoef == 7) {
+          k_pack2d_pitch_ys<T><<<1024, 256, 0, st>>>(cm.ce_curl, cf + 5 * plane2, g.NX, g.NY, tg.NYP, cm.dx, cm.dy);
+          k_pack2d_pitch_ys<T><<<1024, 256, 0, st>>>(cm.ch_curl, cf + 6 * plane2, g.NX, g.NY, tg.NYP, cm.dx, cm.dy);
+          tf.ce_curl_y = cf + 5 * plane2;
+          tf.ch_curl_y = cf + 6 * plane2;
+        }
+        cudaMemsetAsync(cf + ncoef * plane2, 0, kTmTailPad * sizeof(T), st);
         k_pack2d_pitch<T><<<2048, 256, 0, st>>>(fc.Ez, tf.Ez, (long long)g.nshot * g.NX, g.NY, tg.NYP);
         k_pack2d_pitch<T><<<2048, 256, 0, st>>>(fc.Hx, tf.Hx, (long long)g.nshot * g.NX, g.NY, tg.NYP);
         k_pack2d_pitch<T><<<2048, 256, 0, st>>>(fc.Hy, tf.Hy, (long long)g.nshot * g.NX, g.NY, tg.NYP);
@@ -880,12 +923,12 @@ void forward_impl(const ForwardCall<T>& fc) {
         if (tm2d) {
           timed(KK_FWD_H, st, [&] {
             return split_launch(
-                st, ss, pH.interior.nwarps > 0,
-                [&](cudaStream_t q) {
-                  const dim3 gf = tm_grid(pH.frame);
-                  if (R == 1) tm_fwd_h<T, 1><<<gf, wblock, 0, q>>>(b, tf, pH.frame);
-                  else if (R == 2) tm_fwd_h<T, 2><<<gf, wblock, 0, q>>>(b, tf, pH.frame);
-                  else tm_fwd_h<T, 4><<<gf, wblock, 0, q>>>(b, tf, pH.frame);
+                st, ss, pH,
+                [&](cudaStream_t q, const TmGeom& fg) {
+                  const dim3 gf = tm_grid(fg);
+                  if (R == 1) tm_fwd_h<T, 1><<<gf, wblock, 0, q>>>(b, tf, fg);
+                  else if (R == 2) tm_fwd_h<T, 2><<<gf, wblock, 0, q>>>(b, tf, fg);
+                  else tm_fwd_h<T, 4><<<gf, wblock, 0, q>>>(b, tf, fg);
                 },
                 [&](cudaStream_t q) {
                   const dim3 gi = tm_grid(pH.interior);
@@ -896,12 +939,12 @@ void forward_impl(const ForwardCall<T>& fc) {
           });
           timed(KK_FWD_E, st, [&] {
             return split_launch(
-                st, ss, pE.interior.nwarps > 0,
-                [&](cudaStream_t q) {
-                  const dim3 gf = tm_grid(pE.frame);
-                  if (R == 1) tm_fwd_e<T, 1><<<gf, wblock, 0, q>>>(b, tf, pE.frame);
-                  else if (R == 2) tm_fwd_e<T, 2><<<gf, wblock, 0, q>>>(b, tf, pE.frame);
-                  else tm_fwd_e<T, 4><<<gf, wblock, 0, q>>>(b, tf, pE.frame);
+                st, ss, pE,
+                [&](cudaStream_t q, const TmGeom& fg) {
+                  const dim3 gf = tm_grid(fg);
+                  if (R == 1) tm_fwd_e<T, 1><<<gf, wblock, 0, q>>>(b, tf, fg);
+                  else if (R == 2) tm_fwd_e<T, 2><<<gf, wblock, 0, q>>>(b, tf, fg);
+                  else tm_fwd_e<T, 4><<<gf, wblock, 0, q>>>(b, tf, fg);
                 },
                 [&](cudaStream_t q) {
                   const dim3 gi = tm_grid(pE.interior);
@@ -1163,7 +1206,8 @@ void backward_impl(const BackwardCall<T>& bc) {
     memset(&tl, 0, sizeof(tl));
     const long long plane2 = (long long)g.NX * tg.NYP;
     if (ok && tm2d) {
-      T* buf = scratch.get<T>((size_t)(3 * g.nshot + 5) * plane2 * sizeof(T));
+      const int ncoef = cm.dy == cm.dx ? 5 : 7;
+      T* buf = scratch.get<T>(((size_t)(3 * g.nshot + ncoef) * plane2 + kTmTailPad) * sizeof(T));
       ok = buf != nullptr;
       if (ok) {
         tl.Ez = buf;
@@ -1177,6 +1221,15 @@ void backward_impl(const BackwardCall<T>& bc) {
         tl.ce_rhs = cf + 2 * plane2;
         tl.ch_curl = cf + 3 * plane2;
         tl.ch_rhs = cf + 4 * plane2;
+        tl.ce_curl_y = tl.ce_curl;
+        tl.ch_curl_y = tl.ch_curl;
+        if (ncoef == 7) {
+          k_pack2d_pitch_ys<T><<<1024, 256, 0, st>>>(cm.ce_curl, cf + 5 * plane2, g.NX, g.NY, tg.NYP, cm.dx, cm.dy);
+          k_pack2d_pitch_ys<T><<<1024, 256, 0, st>>>(cm.ch_curl, cf + 6 * plane2, g.NX, g.NY, tg.NYP, cm.dx, cm.dy);
+          tl.ce_curl_y = cf + 5 * plane2;
+          tl.ch_curl_y = cf + 6 * plane2;
+        }
+        cudaMemsetAsync(cf + ncoef * plane2, 0, kTmTailPad * sizeof(T), st);
         k_pack2d_pitch<T><<<2048, 256, 0, st>>>(bc.lEz, tl.Ez, (long long)g.nshot * g.NX, g.NY, tg.NYP);
         k_pack2d_pitch<T><<<2048, 256, 0, st>>>(bc.lHx, tl.Hx, (long long)g.nshot * g.NX, g.NY, tg.NYP);
         k_pack2d_pitch<T><<<2048, 256, 0, st>>>(bc.lHy, tl.Hy, (long long)g.nshot * g.NX, g.NY, tg.NYP);
@@ -1197,6 +1250,7 @@ void backward_impl(const BackwardCall<T>& bc) {
         const int bH = R == 1 ? blocks_per_sm(tmi_adj_h<T, 1>) : R == 2 ? blocks_per_sm(tmi_adj_h<T, 2>)
                                                                         : blocks_per_sm(tmi_adj_h<T, 4>);
         pE = tm_plan(tg, g, 2, R, tfc, lean2d, bE);
+        pE.frame.sum_source = 1;   // the adjoint-E frame launch sums the step's source gradient
         pH = tm_plan(tg, g, 3, R, tfc, lean2d, bH, &pt_rows);
         pP = tm_plan(tg, g, 3, R, tfc, false, bH);   // prologue: general kernel everywhere
       }
@@ -1211,10 +1265,11 @@ void backward_impl(const BackwardCall<T>& bc) {
         TiledAdj<T> b = P;
         b.a.k_in_chunk = 0;
         if (tm2d) {
-          const dim3 gP = tm_grid(pP.frame);
-          if (R == 1) tm_adj_h<T, 1, true><<<gP, wblock, 0, st>>>(b, tl, pP.frame);
-          else if (R == 2) tm_adj_h<T, 2, true><<<gP, wblock, 0, st>>>(b, tl, pP.frame);
-          else tm_adj_h<T, 4, true><<<gP, wblock, 0, st>>>(b, tl, pP.frame);
+          const TmGeom& fP = pP.frame;
+          const dim3 gP = tm_grid(fP);
+          if (R == 1) tm_adj_h<T, 1, true><<<gP, wblock, 0, st>>>(b, tl, fP);
+          else if (R == 2) tm_adj_h<T, 2, true><<<gP, wblock, 0, st>>>(b, tl, fP);
+          else tm_adj_h<T, 4, true><<<gP, wblock, 0, st>>>(b, tl, fP);
         } else {
           if (R == 1) k3_adj_h<T, 1, true><<<grid, 256, 0, st>>>(b);
           else if (R == 2) k3_adj_h<T, 2, true><<<grid, 256, 0, st>>>(b);
@@ -1227,19 +1282,19 @@ void backward_impl(const BackwardCall<T>& bc) {
         b.a.k_in_chunk = k;
         if (want_model && img_blocks > 0) {
           if (tm2d)
-            timed(KK_IMAGE, st, [&] { launch_tm_image<T>(kind, a.e_only != 0, a.acc64 != 0, img_blocks, st, b.a, tl.Ez, tg); });
+            timed(KK_IMAGE, st, [&] { launch_tm_image<T>(kind, a.e_only != 0, a.acc64 != 0, st, b.a, tl.Ez, tg); });
           else
             timed(KK_IMAGE, st, [&] { k_image<T><<<img_blocks, 256, 0, st>>>(b.a, lamx, lamy, lamz); });
         }
         if (tm2d) {
           timed(KK_ADJ_E, st, [&] {
             return split_launch(
-                st, ss, pE.interior.nwarps > 0,
-                [&](cudaStream_t q) {
-                  const dim3 gf = tm_grid(pE.frame);
-                  if (R == 1) tm_adj_e<T, 1><<<gf, wblock, 0, q>>>(b, tl, pE.frame);
-                  else if (R == 2) tm_adj_e<T, 2><<<gf, wblock, 0, q>>>(b, tl, pE.frame);
-                  else tm_adj_e<T, 4><<<gf, wblock, 0, q>>>(b, tl, pE.frame);
+                st, ss, pE,
+                [&](cudaStream_t q, const TmGeom& fg) {
+                  const dim3 gf = tm_grid(fg);
+                  if (R == 1) tm_adj_e<T, 1><<<gf, wblock, 0, q>>>(b, tl, fg);
+                  else if (R == 2) tm_adj_e<T, 2><<<gf, wblock, 0, q>>>(b, tl, fg);
+                  else tm_adj_e<T, 4><<<gf, wblock, 0, q>>>(b, tl, fg);
                 },
                 [&](cudaStream_t q) {
                   const dim3 gi = tm_grid(pE.interior);
@@ -1250,12 +1305,12 @@ void backward_impl(const BackwardCall<T>& bc) {
           });
           timed(KK_ADJ_H, st, [&] {
             return split_launch(
-                st, ss, pH.interior.nwarps > 0,
-                [&](cudaStream_t q) {
-                  const dim3 gf = tm_grid(pH.frame);
-                  if (R == 1) tm_adj_h<T, 1, false><<<gf, wblock, 0, q>>>(b, tl, pH.frame);
-                  else if (R == 2) tm_adj_h<T, 2, false><<<gf, wblock, 0, q>>>(b, tl, pH.frame);
-                  else tm_adj_h<T, 4, false><<<gf, wblock, 0, q>>>(b, tl, pH.frame);
+                st, ss, pH,
+                [&](cudaStream_t q, const TmGeom& fg) {
+                  const dim3 gf = tm_grid(fg);
+                  if (R == 1) tm_adj_h<T, 1, false><<<gf, wblock, 0, q>>>(b, tl, fg);
+                  else if (R == 2) tm_adj_h<T, 2, false><<<gf, wblock, 0, q>>>(b, tl, fg);
+                  else tm_adj_h<T, 4, false><<<gf, wblock, 0, q>>>(b, tl, fg);
                 },
                 [&](cudaStream_t q) {
                   const dim3 gi = tm_grid(pH.interior);
