@@ -18,7 +18,6 @@ PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 OUT = PKG / "lib" / "libdeepgpr_b200.so"
 SOURCES = ("fdtd_api.cu",)
-HEADERS = ("fdtd_common.cuh", "fdtd_forward.cuh", "fdtd_adjoint.cuh", "fdtd_tiled.cuh", "fdtd_tiled_adj.cuh", "fdtd_tm2d.cuh")
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -39,7 +38,8 @@ def stale() -> bool:
     if not OUT.is_file():
         return True
     t = OUT.stat().st_mtime
-    return any((CSRC / f).stat().st_mtime > t for f in SOURCES + HEADERS)
+    deps = [CSRC / f for f in SOURCES] + sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.h"))
+    return any(f.stat().st_mtime > t for f in deps)
 
 
 def build(force: bool = False, verbose: bool = False) -> Path:

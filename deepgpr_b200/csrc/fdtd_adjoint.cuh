@@ -38,6 +38,7 @@ struct AdjArgs {
   Grid g;
   T dx, dy, dz;
   T inv_dx, inv_dy, inv_dz;         // 1/spacing as the reference forms it
+  FixedDiv<T> ddt;                  // division by dt (imaging condition)
   int dy_eq, dz_eq;
   T *lEx, *lEy, *lEz, *lHx, *lHy, *lHz;
   const T *ce_hist, *ce_curl, *ce_rhs, *ch_curl, *ch_rhs;
@@ -438,8 +439,8 @@ __global__ void __launch_bounds__(kBlock) k_adj_h(AdjArgs<T> a) {
     if (it + w > a.nt) w = a.nt - it;
     wgt = T(w);
     pec_ok = a.sigma[c] <= Phys<T>::pec();
-    dca_e = Phys<T>::eps0() * (T(1) - ca) * cbv / a.dt;
-    dcb_e = -Phys<T>::eps0() * cbv * cbv / a.dt;
+    dca_e = div_fixed(Phys<T>::eps0() * (T(1) - ca) * cbv, a.ddt);
+    dcb_e = div_fixed(-Phys<T>::eps0() * cbv * cbv, a.ddt);
     dca_s = T(-0.5) * (T(1) + ca) * cbv;
     dcb_s = T(-0.5) * cbv * cbv;
   }

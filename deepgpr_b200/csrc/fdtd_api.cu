@@ -22,7 +22,7 @@
 #include <string>
 #include <vector>
 
-#include "fdtd_tm2d.cuh"
+#include "fdtd_3d.cuh"
 
 #define DGB_API extern "C" __attribute__((visibility("default")))
 
@@ -548,6 +548,80 @@ int split_launch(cudaStream_t st, const StreamSet* ss, const TmPlan& pl, FrameFn
 
 dim3 tm_grid(const TmGeom& tg) { return dim3((unsigned)std::max<long long>(1, (tg.nwarps + TM_WARPS - 1) / TM_WARPS)); }
 
+// 3D working copy: z pitch, strips, y tiles and x chunks.  The chunking keeps
+// the last wave of CTAs nearly full (occupancy of the forward H kernel).
+K3Geom k3_layout(const Grid& g) {
+  K3Geom kg;
+  memset(&kg, 0, sizeof(kg));
+  kg.zp = (g.NZ + 31) / 32 * 32;
+  kg.nzs = (g.NZ + K3W - 1) / K3W;
+  kg.nyt = (g.NY + K3_WARPS - 1) / K3_WARPS;
+  int blocks = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k3v_fwd_h<float, 2, true>, 32 * K3_WARPS, 0) !=
+          cudaSuccess ||
+      blocks < 1) {
+    cudaGetLastError();
+    blocks = 4;
+  }
+  const double resident = (double)sm_count() * blocks;
+  const long long per = (long long)g.nshot * kg.nzs * kg.nyt;
+  int best = 1;
+  double best_eff = -1.0;
+  for (int n = 1; n <= std::max(1, std::min(64, g.NX / 16)); ++n) {
+    const int xc = (g.NX + n - 1) / n;
+    const int nch = (g.NX + xc - 1) / xc;
+    const double nb = (double)per * nch;
+    const double waves = std::ceil(nb / resident);
+    const double eff = nb / (waves * resident) * (double)xc / (xc + 3.0);
+    if (eff > best_eff + 1e-3) {
+      best_eff = eff;
+      best = n;
+    }
+  }
+  kg.xc = (g.NX + best - 1) / best;
+  kg.nchunk = (g.NX + kg.xc - 1) / kg.xc;
+  kg.nblocks = per * kg.nchunk;
+  return kg;
+}
+
+// Allocates the 3D working copy and packs the fields and coefficients into it.
+template <typename T, typename Alloc, typename CM>
+bool k3_alloc_pack(Alloc& scratch, const Grid& g, const K3Geom& kg, const CM& cm, cudaStream_t st, K3Buf<T>& kf,
+                   const T* Ex, const T* Ey, const T* Ez, const T* Hx, const T* Hy, const T* Hz) {
+  const long long rows = (long long)g.NX * g.NY;
+  const long long plane = rows * kg.zp;
+  T* buf = scratch.template get<T>(((size_t)(6 * g.nshot + 5) * plane + 64) * sizeof(T));
+  if (!buf) return false;
+  T* fields[6];
+  const T* srcs[6] = {Ex, Ey, Ez, Hx, Hy, Hz};
+  for (int q = 0; q < 6; ++q) {
+    fields[q] = buf + (long long)q * g.nshot * plane;
+    k_pack_rows<T><<<2048, 256, 0, st>>>(srcs[q], fields[q], rows * g.nshot, g.NZ, kg.zp);
+  }
+  kf.Ex = fields[0]; kf.Ey = fields[1]; kf.Ez = fields[2];
+  kf.Hx = fields[3]; kf.Hy = fields[4]; kf.Hz = fields[5];
+  T* cf = buf + 6LL * g.nshot * plane;
+  const T* coef[5] = {cm.ce_hist, cm.ce_curl, cm.ce_rhs, cm.ch_curl, cm.ch_rhs};
+  for (int q = 0; q < 5; ++q) k_pack_rows<T><<<1024, 256, 0, st>>>(coef[q], cf + q * plane, rows, g.NZ, kg.zp);
+  kf.ce_hist = cf;
+  kf.ce_curl = cf + plane;
+  kf.ce_rhs = cf + 2 * plane;
+  kf.ch_curl = cf + 3 * plane;
+  kf.ch_rhs = cf + 4 * plane;
+  cudaMemsetAsync(cf + 5 * plane, 0, 64 * sizeof(T), st);
+  return cuda_ok(cudaGetLastError(), "3D pack");
+}
+
+template <typename T>
+bool k3_unpack(const Grid& g, const K3Geom& kg, cudaStream_t st, const K3Buf<T>& kf, T* Ex, T* Ey, T* Ez, T* Hx,
+               T* Hy, T* Hz) {
+  const long long rows = (long long)g.NX * g.NY * g.nshot;
+  const T* srcs[6] = {kf.Ex, kf.Ey, kf.Ez, kf.Hx, kf.Hy, kf.Hz};
+  T* dsts[6] = {Ex, Ey, Ez, Hx, Hy, Hz};
+  for (int q = 0; q < 6; ++q) k_unpack_rows<T><<<2048, 256, 0, st>>>(srcs[q], dsts[q], rows, g.NZ, kg.zp);
+  return cuda_ok(cudaGetLastError(), "3D unpack");
+}
+
 template <typename T>
 TmFaces tm_faces(const Face<T>* eF, const Face<T>* hF, bool cpml) {
   TmFaces f;
@@ -633,11 +707,10 @@ HBox make_box(const Grid& g, bool physical, const int* p) {
 
 long long ntiles_of(const Grid& g) { return ((long long)g.cells + kBlock - 1) / kBlock; }
 
-// FP8 scale tiles: one per (x plane, CTA tile) of the 3D forward kernels, one
-// per (row, 32-column strip) of the 2D TM kernels.
+// FP8 scale tiles: one per (x plane, y row, 32 z columns) in 3D, one per
+// (row, 32-column strip) in 2D TM.
 long long fp8_tiles(const Grid& g, bool tm2d) {
-  return (long long)g.NX * (tm2d ? (long long)(g.NY + TMW - 1) / TMW
-                                 : (long long)((g.NY + TY - 1) / TY) * ((g.NZ + TZ - 1) / TZ));
+  return (long long)g.NX * (tm2d ? (long long)(g.NY + TMW - 1) / TMW : (long long)g.NY * ((g.NZ + 31) / 32));
 }
 
 // FP8 history buffer: payload (1 byte per value) padded to 256 bytes, then
@@ -804,6 +877,9 @@ void forward_impl(const ForwardCall<T>& fc) {
     a.dx = cm.dx;
     a.dy = cm.dy;
     a.dz = cm.dz;
+    a.ddx = fixed_div(cm.dx);
+    a.ddy = fixed_div(cm.dy);
+    a.ddz = fixed_div(cm.dz);
     a.dy_eq = cm.dy == cm.dx;
     a.dz_eq = cm.dz == cm.dx;
     a.Ex = fc.Ex; a.Ey = fc.Ey; a.Ez = fc.Ez;
@@ -850,12 +926,15 @@ void forward_impl(const ForwardCall<T>& fc) {
     if (tm2d) tg = tm_layout(g);
     // sources of an invalid component inject nothing (deepgpr_cpu.c:650)
     std::vector<char> src_any, rcv_any;
+    const unsigned char *src_rows = nullptr, *rcv_rows = nullptr;
     if (ok && fc.src_comp >= 0 && fc.src_comp <= 2)
       ok = build_pointset(fc.src_loc, g.nshot, fc.nsrc, g, st, scratch, &P.src, &a.src, "source", kErrSourceRange,
-                          tm2d ? &tg.src_rows : nullptr, tm2d ? &src_any : nullptr);
+                          &src_rows, tm2d ? &src_any : nullptr);
     if (ok)
       ok = build_pointset(fc.rx_loc, g.nshot, fc.nrx, g, st, scratch, &P.rcv, &a.rcv, "receiver", kErrReceiverRange,
-                          tm2d ? &tg.rcv_rows : nullptr, tm2d ? &rcv_any : nullptr);
+                          &rcv_rows, tm2d ? &rcv_any : nullptr);
+    tg.src_rows = src_rows;
+    tg.rcv_rows = rcv_rows;
     // rows with a source or receiver of any shot go to the general (frame) kernels
     std::vector<char> pt_rows(tm2d ? g.NX : 0, 0);
     for (int i = 0; i < (int)pt_rows.size(); ++i)
@@ -896,6 +975,20 @@ void forward_impl(const ForwardCall<T>& fc) {
         k_pack2d_pitch<T><<<2048, 256, 0, st>>>(fc.Hy, tf.Hy, (long long)g.nshot * g.NX, g.NY, tg.NYP);
         ok = cuda_ok(cudaGetLastError(), "pack");
       }
+    }
+    // 3D: z-pitched working copy of the fields and coefficients
+    K3Buf<T> kf;
+    memset(&kf, 0, sizeof(kf));
+    K3Geom kg;
+    memset(&kg, 0, sizeof(kg));
+    const bool eq3 = cm.dy == cm.dx && cm.dz == cm.dx;
+    if (ok && !tm2d) {
+      kg = k3_layout(g);
+      kg.src_rows = src_rows;
+      kg.rcv_rows = rcv_rows;
+      const int* pf = cm.p;   // face thicknesses x0, xm, y0, ym, z0, zm
+      kg.cpml_single = g.NX >= pf[0] + pf[1] + 4 && g.NY >= pf[2] + pf[3] + 4 && g.NZ >= pf[4] + pf[5] + 4;
+      ok = k3_alloc_pack(scratch, g, kg, cm, st, kf, fc.Ex, fc.Ey, fc.Ez, fc.Hx, fc.Hy, fc.Hz);
     }
     if (ok) {
       a.ctrl = ctrl;
@@ -954,15 +1047,28 @@ void forward_impl(const ForwardCall<T>& fc) {
                 });
           });
         } else {
+          const dim3 g3((unsigned)kg.nblocks), b3(32, K3_WARPS);
           timed(KK_FWD_H, st, [&] {
-            if (R == 1) k3_fwd_h<T, 1><<<grid, 256, 0, st>>>(b);
-            else if (R == 2) k3_fwd_h<T, 2><<<grid, 256, 0, st>>>(b);
-            else k3_fwd_h<T, 4><<<grid, 256, 0, st>>>(b);
+            if (eq3) {
+              if (R == 1) k3v_fwd_h<T, 1, true><<<g3, b3, 0, st>>>(b, kf, kg);
+              else if (R == 2) k3v_fwd_h<T, 2, true><<<g3, b3, 0, st>>>(b, kf, kg);
+              else k3v_fwd_h<T, 4, true><<<g3, b3, 0, st>>>(b, kf, kg);
+            } else {
+              if (R == 1) k3v_fwd_h<T, 1, false><<<g3, b3, 0, st>>>(b, kf, kg);
+              else if (R == 2) k3v_fwd_h<T, 2, false><<<g3, b3, 0, st>>>(b, kf, kg);
+              else k3v_fwd_h<T, 4, false><<<g3, b3, 0, st>>>(b, kf, kg);
+            }
           });
           timed(KK_FWD_E, st, [&] {
-            if (R == 1) k3_fwd_e<T, 1><<<grid, 256, 0, st>>>(b);
-            else if (R == 2) k3_fwd_e<T, 2><<<grid, 256, 0, st>>>(b);
-            else k3_fwd_e<T, 4><<<grid, 256, 0, st>>>(b);
+            if (eq3) {
+              if (R == 1) k3v_fwd_e<T, 1, true><<<g3, b3, 0, st>>>(b, kf, kg);
+              else if (R == 2) k3v_fwd_e<T, 2, true><<<g3, b3, 0, st>>>(b, kf, kg);
+              else k3v_fwd_e<T, 4, true><<<g3, b3, 0, st>>>(b, kf, kg);
+            } else {
+              if (R == 1) k3v_fwd_e<T, 1, false><<<g3, b3, 0, st>>>(b, kf, kg);
+              else if (R == 2) k3v_fwd_e<T, 2, false><<<g3, b3, 0, st>>>(b, kf, kg);
+              else k3v_fwd_e<T, 4, false><<<g3, b3, 0, st>>>(b, kf, kg);
+            }
           });
         }
       };
@@ -973,6 +1079,7 @@ void forward_impl(const ForwardCall<T>& fc) {
         k_unpack2d_pitch<T><<<2048, 256, 0, st>>>(tf.Hy, fc.Hy, (long long)g.nshot * g.NX, g.NY, tg.NYP);
         ok = cuda_ok(cudaGetLastError(), "unpack");
       }
+      if (ok && !tm2d) ok = k3_unpack(g, kg, st, kf, fc.Ex, fc.Ey, fc.Ez, fc.Hx, fc.Hy, fc.Hz);
       if (ok && e_only) {
         // closing E^nt frame into R_saved (deepgpr_cpu.c:1919-1930)
         const long long bc = a.box.cells();
@@ -1097,6 +1204,7 @@ void backward_impl(const BackwardCall<T>& bc) {
     a.dx = cm.dx;
     a.dy = cm.dy;
     a.dz = cm.dz;
+    a.ddt = fixed_div(cm.dt);
     a.inv_dx = T(1) / cm.dx;
     a.inv_dy = T(1) / cm.dy;
     a.inv_dz = T(1) / cm.dz;
@@ -1491,6 +1599,50 @@ DGB_API void dgb_forward_noalloc(DGB_FWD_PARAMS(float)) {
 DGB_API void backward(DGB_BWD_PARAMS(float)) { DGB_BACKWARD_BODY(float); }
 DGB_API void dgb_forward_f64(DGB_FWD_PARAMS(double)) { DGB_FORWARD_BODY(double); }
 DGB_API void dgb_backward_f64(DGB_BWD_PARAMS(double)) { DGB_BACKWARD_BODY(double); }
+
+// Exhaustive check of div_fixed against the division operator for one divisor.
+__global__ void k_check_fixed_div(FixedDiv<float> d, unsigned long long* bad, unsigned* first) {
+  const unsigned long long nth = (unsigned long long)gridDim.x * blockDim.x;
+  unsigned long long cnt = 0;
+  unsigned lowest = 0xffffffffu;
+  for (unsigned long long u = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; u < (1ull << 32); u += nth) {
+    const float a = __uint_as_float((unsigned)u);
+    if (__float_as_uint(div_fixed(a, d)) != __float_as_uint(a / d.b)) {
+      ++cnt;
+      lowest = min(lowest, (unsigned)u);
+    }
+  }
+  if (cnt) {
+    atomicAdd(bad, cnt);
+    atomicMin(first, lowest);
+  }
+}
+
+// Diagnostic: the number of float dividends (all 2^32 bit patterns) whose
+// correctly rounded division by `divisor` through the solver's fixed-divisor
+// path differs from the division operator, and the lowest such bit pattern.
+// Runs synchronously on the current device; returns 0, or -1 with the error.
+DGB_API int dgb_check_fixed_division(float divisor, unsigned long long* mismatches, unsigned* first_bad) {
+  void* buf = nullptr;
+  if (!cuda_ok(cudaMalloc(&buf, 16), "dgb_check_fixed_division: cudaMalloc")) return -1;
+  unsigned long long* bad = static_cast<unsigned long long*>(buf);
+  unsigned* first = reinterpret_cast<unsigned*>(bad + 1);
+  const unsigned init[4] = {0u, 0u, 0xffffffffu, 0u};
+  bool ok = cuda_ok(cudaMemcpy(buf, init, 16, cudaMemcpyHostToDevice), "dgb_check_fixed_division: upload");
+  if (ok) {
+    k_check_fixed_div<<<sm_count() * 8, 256>>>(fixed_div(divisor), bad, first);
+    ok = cuda_ok(cudaGetLastError(), "dgb_check_fixed_division: launch");
+  }
+  unsigned out[4] = {0u, 0u, 0u, 0u};
+  if (ok) ok = cuda_ok(cudaMemcpy(out, buf, 16, cudaMemcpyDeviceToHost), "dgb_check_fixed_division: download");
+  cudaFree(buf);
+  if (!ok) return -1;
+  unsigned long long n = 0;
+  memcpy(&n, out, sizeof(n));
+  if (mismatches) *mismatches = n;
+  if (first_bad) *first_bad = out[2];
+  return 0;
+}
 
 DGB_API int deepgpr_abi_version(void) { return 6; }
 DGB_API int deepgpr_supports_error_reporting(void) { return 1; }

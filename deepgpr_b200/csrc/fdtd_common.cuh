@@ -17,6 +17,8 @@
 #include <cuda_fp8.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 namespace dg {
 
 constexpr int kBlock = 256;          // threads per CTA in every grid kernel
@@ -167,6 +169,90 @@ struct Face {
   T* w2;          // adjoint only: psi2-shaped
   int p;
 };
+
+// ---------------------------------------------------------------------------
+// Division by a divisor shared by many dividends, correctly rounded.
+//
+// The CPML recurrences divide a difference by the spacing (d = dv / h) in
+// every boundary cell, the imaging condition divides by dt and the E-only
+// history divides every shot's value of a cell by the cell's coefficient.
+// For single precision the quotient is computed from y = RN(1/b) -- worked
+// out on the host in double precision for a spacing or dt (that rounding
+// cannot fall on a float rounding boundary, so y is the correctly rounded
+// reciprocal), or by __frcp_rn for a per-cell divisor -- by
+//   q0 = RN(a y),  q_{k+1} = RN(q_k + RN(a - b q_k) y)   (FMA),
+// Markstein's correction (P. Markstein, "Computation of elementary functions
+// on the IBM RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990).  q0
+// is within two ulps of a/b; the first correction leaves an error of a few
+// 2^-23 ulp before rounding, so q1 is within one ulp; Markstein's theorem (y
+// within half an ulp of 1/b, q within one ulp of a/b, a - b q exact, no
+// underflow or overflow) then makes q2 = RN(a/b).  The FMA path takes
+// divisors in [2^-120, 2^120] and dividends with |a| >= 2^-100 (so that
+// a - b q, a multiple of about ulp(a) 2^-24, is representable) and
+// 2^-100 <= |a/b| <= 2^100; zeros return a (a / b for b > 0) and every
+// other dividend uses the division operator.  The exported check
+// dgb_check_fixed_division compares it with the division operator over all
+// 2^32 dividends of a divisor.
+// ---------------------------------------------------------------------------
+template <typename T>
+struct FixedDiv {
+  T b, y;      // divisor, RN(1 / b)
+  T lo, hi;    // dividends with lo <= |a| <= hi take the FMA path (lo > hi: never)
+};
+
+template <typename T>
+inline FixedDiv<T> fixed_div(T b) {
+  FixedDiv<T> d;
+  d.b = b;
+  d.y = T(1.0 / (double)b);
+  const bool ok = sizeof(T) == 4 && b >= T(0x1p-120) && b <= T(0x1p120);
+  d.lo = ok ? std::max(T(0x1p-100), b * T(0x1p-100)) : T(1);
+  d.hi = ok ? std::min(T(0x1p100), b * T(0x1p100)) : T(0);
+  return d;
+}
+
+// The same for a divisor known only on the device and shared by several
+// dividends (y from the correctly rounded reciprocal __frcp_rn).
+template <typename T>
+__device__ __forceinline__ FixedDiv<T> fixed_div_dev(T b) {
+  FixedDiv<T> d;
+  d.b = b;
+  if constexpr (sizeof(T) == 4) {
+    d.y = __frcp_rn(b);
+    const bool ok = b >= 0x1p-120f && b <= 0x1p120f;
+    d.lo = ok ? fmaxf(0x1p-100f, b * 0x1p-100f) : 1.0f;
+    d.hi = ok ? fminf(0x1p100f, b * 0x1p100f) : 0.0f;
+  } else {
+    d.y = T(1) / b;
+    d.lo = T(1);
+    d.hi = T(0);
+  }
+  return d;
+}
+
+// The division operator out of line: a call is never evaluated
+// speculatively, so the rare dividends outside the FMA range do not make
+// every lane pay for a full division.
+__device__ __noinline__ inline float div_operator(float a, float b) { return a / b; }
+
+template <typename T>
+__device__ __forceinline__ T div_fixed(T a, const FixedDiv<T>& d) {
+  if constexpr (sizeof(T) == 4) {
+    const float m = fabsf(a);
+    // zeros: a / b == a for b > 0 (y > 0); the FMA path would lose the sign of -0
+    if ((m >= d.lo && m <= d.hi) || (m == 0.0f && d.y > 0.0f)) {
+      float q = a * d.y;
+      float r = fmaf(-d.b, q, a);
+      q = fmaf(r, d.y, q);
+      r = fmaf(-d.b, q, a);
+      q = fmaf(r, d.y, q);
+      return m == 0.0f ? a : q;
+    }
+    return div_operator(a, d.b);
+  } else {
+    return a / d.b;
+  }
+}
 
 template <typename T>
 struct Prof {

@@ -18,6 +18,7 @@ template <typename T>
 struct FwdArgs {
   Grid g;
   T dx, dy, dz;
+  FixedDiv<T> ddx, ddy, ddz;        // division by dx, dy, dz (CPML differences, curl scaling)
   int dy_eq, dz_eq;                 // dy == dx, dz == dx (selects the curl scaling)
   T *Ex, *Ey, *Ez, *Hx, *Hy, *Hz;
   const T *ce_hist, *ce_curl, *ce_rhs, *ch_curl, *ch_rhs;
@@ -143,39 +144,39 @@ __global__ void __launch_bounds__(kBlock) k_fwd_h(FwdArgs<T> a) {
         if (axis == 0) {
           if (k < g.NZ - 1) {
             const long long pi = psi_index(psi_dims_h(g, 0, 1, F.p), 0, s, q, i, j, k);
-            const T d = dEz_dx / a.dx, ph = F.psi1[pi];
+            const T d = div_fixed(dEz_dx, a.ddx), ph = F.psi1[pi];
             hy += up * (pr.ra1 * d + pr.rb * ph);
             F.psi1[pi] = pr.re * ph - pr.rf * d;
           }
           if (j < g.NY - 1) {
             const long long pi = psi_index(psi_dims_h(g, 0, 2, F.p), 0, s, q, i, j, k);
-            const T d = dEy_dx / a.dx, ph = F.psi2[pi];
+            const T d = div_fixed(dEy_dx, a.ddx), ph = F.psi2[pi];
             hz -= up * (pr.ra1 * d + pr.rb * ph);
             F.psi2[pi] = pr.re * ph - pr.rf * d;
           }
         } else if (axis == 1) {
           if (k < g.NZ - 1) {
             const long long pi = psi_index(psi_dims_h(g, 1, 1, F.p), 1, s, q, i, j, k);
-            const T d = dEz_dy / a.dy, ph = F.psi1[pi];
+            const T d = div_fixed(dEz_dy, a.ddy), ph = F.psi1[pi];
             hx -= up * (pr.ra1 * d + pr.rb * ph);
             F.psi1[pi] = pr.re * ph - pr.rf * d;
           }
           if (i < g.NX - 1) {
             const long long pi = psi_index(psi_dims_h(g, 1, 2, F.p), 1, s, q, i, j, k);
-            const T d = dEx_dy / a.dy, ph = F.psi2[pi];
+            const T d = div_fixed(dEx_dy, a.ddy), ph = F.psi2[pi];
             hz += up * (pr.ra1 * d + pr.rb * ph);
             F.psi2[pi] = pr.re * ph - pr.rf * d;
           }
         } else {
           if (j < g.NY - 1) {
             const long long pi = psi_index(psi_dims_h(g, 2, 1, F.p), 2, s, q, i, j, k);
-            const T d = dEy_dz / a.dz, ph = F.psi1[pi];
+            const T d = div_fixed(dEy_dz, a.ddz), ph = F.psi1[pi];
             hx += up * (pr.ra1 * d + pr.rb * ph);
             F.psi1[pi] = pr.re * ph - pr.rf * d;
           }
           if (i < g.NX - 1) {
             const long long pi = psi_index(psi_dims_h(g, 2, 2, F.p), 2, s, q, i, j, k);
-            const T d = dEx_dz / a.dz, ph = F.psi2[pi];
+            const T d = div_fixed(dEx_dz, a.ddz), ph = F.psi2[pi];
             hy -= up * (pr.ra1 * d + pr.rb * ph);
             F.psi2[pi] = pr.re * ph - pr.rf * d;
           }
@@ -271,39 +272,39 @@ __global__ void __launch_bounds__(kBlock) k_fwd_e(FwdArgs<T> a) {
           if (axis == 0) {
             if (j < g.NY - 1) {
               const long long pi = psi_index(psi_dims_e(g, 0, 1, F.p), 0, s, q, i, j, k);
-              const T d = dHz_dx / a.dx, ph = F.psi1[pi];
+              const T d = div_fixed(dHz_dx, a.ddx), ph = F.psi1[pi];
               ey -= cb * (pr.ra1 * d + pr.rb * ph);
               F.psi1[pi] = pr.re * ph - pr.rf * d;
             }
             if (k < g.NZ - 1) {
               const long long pi = psi_index(psi_dims_e(g, 0, 2, F.p), 0, s, q, i, j, k);
-              const T d = dHy_dx / a.dx, ph = F.psi2[pi];
+              const T d = div_fixed(dHy_dx, a.ddx), ph = F.psi2[pi];
               ez += cb * (pr.ra1 * d + pr.rb * ph);
               F.psi2[pi] = pr.re * ph - pr.rf * d;
             }
           } else if (axis == 1) {
             if (i < g.NX - 1) {
               const long long pi = psi_index(psi_dims_e(g, 1, 1, F.p), 1, s, q, i, j, k);
-              const T d = dHz_dy / a.dy, ph = F.psi1[pi];
+              const T d = div_fixed(dHz_dy, a.ddy), ph = F.psi1[pi];
               ex += cb * (pr.ra1 * d + pr.rb * ph);
               F.psi1[pi] = pr.re * ph - pr.rf * d;
             }
             if (k < g.NZ - 1) {
               const long long pi = psi_index(psi_dims_e(g, 1, 2, F.p), 1, s, q, i, j, k);
-              const T d = dHx_dy / a.dy, ph = F.psi2[pi];
+              const T d = div_fixed(dHx_dy, a.ddy), ph = F.psi2[pi];
               ez -= cb * (pr.ra1 * d + pr.rb * ph);
               F.psi2[pi] = pr.re * ph - pr.rf * d;
             }
           } else {
             if (i < g.NX - 1) {
               const long long pi = psi_index(psi_dims_e(g, 2, 1, F.p), 2, s, q, i, j, k);
-              const T d = dHy_dz / a.dz, ph = F.psi1[pi];
+              const T d = div_fixed(dHy_dz, a.ddz), ph = F.psi1[pi];
               ex -= cb * (pr.ra1 * d + pr.rb * ph);
               F.psi1[pi] = pr.re * ph - pr.rf * d;
             }
             if (j < g.NY - 1) {
               const long long pi = psi_index(psi_dims_e(g, 2, 2, F.p), 2, s, q, i, j, k);
-              const T d = dHx_dz / a.dz, ph = F.psi2[pi];
+              const T d = div_fixed(dHx_dz, a.ddz), ph = F.psi2[pi];
               ey += cb * (pr.ra1 * d + pr.rb * ph);
               F.psi2[pi] = pr.re * ph - pr.rf * d;
             }

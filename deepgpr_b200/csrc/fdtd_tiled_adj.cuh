@@ -440,8 +440,9 @@ __global__ void __launch_bounds__(256) k_image(AdjArgs<T> a, const T* lam_x, con
   if (it + w > a.nt) w = a.nt - it;
   const T wgt = T(w);
   const bool pec_ok = a.sigma[c] <= Phys<T>::pec();
-  const T dca_e = Phys<T>::eps0() * (T(1) - ca) * cbv / a.dt;
-  const T dcb_e = -Phys<T>::eps0() * cbv * cbv / a.dt;
+  const T dca_e = div_fixed(Phys<T>::eps0() * (T(1) - ca) * cbv, a.ddt);
+  const T dcb_e = div_fixed(-Phys<T>::eps0() * cbv * cbv, a.ddt);
+  const FixedDiv<T> dcb = fixed_div_dev(cbv);   // shared by the shots
   const T dca_s = T(-0.5) * (T(1) + ca) * cbv;
   const T dcb_s = T(-0.5) * cbv * cbv;
   const bool dex = upd_ex(g, i, j, k), dey = upd_ey(g, i, j, k), dez = upd_ez(g, i, j, k);
@@ -469,7 +470,7 @@ __global__ void __launch_bounds__(256) k_image(AdjArgs<T> a, const T* lam_x, con
         const T nxt = slot + 1 < a.nt_saved ? hist_load<T>(a.E_saved, hix + a.frame, a.kind, 1.0f)
                                             : hist_load<T>(a.R_saved, q * a.frame + s * bc + hidx, a.kind, 1.0f);
         const T aeff = du ? ca : T(1);
-        rhs = cbv != T(0) ? (nxt - aeff * eo) / cbv : T(0);
+        rhs = cbv != T(0) ? div_fixed(nxt - aeff * eo, dcb) : T(0);
       }
       T lam = fc == 0 ? lam_x[lf] : (fc == 1 ? lam_y[lf] : lam_z[lf]);
       if (eo == T(0) && rhs == T(0)) lam = T(0);

@@ -228,7 +228,7 @@ __device__ __forceinline__ void tm_fwd_h_body(const TiledFwd<T>& P, const TmBuf<
           const Face<T>& F = a.hF[fc];
           const Prof<T> pr = prof(F, qq);
           const long long pi = ((long long)s * F.p + qq) * NY + j;
-          const T d = dEz_dx / a.dx, ph = F.psi1[pi];
+          const T d = div_fixed(dEz_dx, a.ddx), ph = F.psi1[pi];
           hyv += up * (pr.ra1 * d + pr.rb * ph);
           F.psi1[pi] = pr.re * ph - pr.rf * d;
         }
@@ -239,7 +239,7 @@ __device__ __forceinline__ void tm_fwd_h_body(const TiledFwd<T>& P, const TmBuf<
           const Face<T>& F = a.hF[2 + fc];
           const Prof<T> pr = prof(F, qq);
           const long long pi = ((long long)s * NX + i) * F.p + qq;
-          const T d = dEz_dy / a.dy, ph = F.psi1[pi];
+          const T d = div_fixed(dEz_dy, a.ddy), ph = F.psi1[pi];
           hxv -= up * (pr.ra1 * d + pr.rb * ph);
           F.psi1[pi] = pr.re * ph - pr.rf * d;
         }
@@ -357,7 +357,7 @@ __device__ __forceinline__ void tm_fwd_e_body(const TiledFwd<T>& P, const TmBuf<
           const Face<T>& F = a.eF[fc];
           const Prof<T> pr = prof(F, qq);
           const long long pi = ((long long)s * (F.p + 1) + qq) * NY + j;
-          const T d = dHy_dx / a.dx, ph = F.psi2[pi];
+          const T d = div_fixed(dHy_dx, a.ddx), ph = F.psi2[pi];
           ez += cb * (pr.ra1 * d + pr.rb * ph);
           F.psi2[pi] = pr.re * ph - pr.rf * d;
         }
@@ -368,7 +368,7 @@ __device__ __forceinline__ void tm_fwd_e_body(const TiledFwd<T>& P, const TmBuf<
           const Face<T>& F = a.eF[2 + fc];
           const Prof<T> pr = prof(F, qq);
           const long long pi = ((long long)s * NX + i) * (F.p + 1) + qq;
-          const T d = dHx_dy / a.dy, ph = F.psi2[pi];
+          const T d = div_fixed(dHx_dy, a.ddy), ph = F.psi2[pi];
           ez -= cb * (pr.ra1 * d + pr.rb * ph);
           F.psi2[pi] = pr.re * ph - pr.rf * d;
         }
@@ -763,8 +763,9 @@ __global__ void __launch_bounds__(kImageThreads) tm_image(AdjArgs<T> a, const T*
   if (it + w > a.nt) w = a.nt - it;
   const T wgt = T(w);
   const bool pec_ok = a.sigma[c] <= Phys<T>::pec();
-  const T dca_e = Phys<T>::eps0() * (T(1) - ca) * cbv / a.dt;
-  const T dcb_e = -Phys<T>::eps0() * cbv * cbv / a.dt;
+  const T dca_e = div_fixed(Phys<T>::eps0() * (T(1) - ca) * cbv, a.ddt);
+  const T dcb_e = div_fixed(-Phys<T>::eps0() * cbv * cbv, a.ddt);
+  const FixedDiv<T> dcb = fixed_div_dev(cbv);   // shared by the shots
   const T dca_s = T(-0.5) * (T(1) + ca) * cbv;
   const T dcb_s = T(-0.5) * cbv * cbv;
   const bool dez = upd_ez(g, i, j, 0);
@@ -781,7 +782,7 @@ __global__ void __launch_bounds__(kImageThreads) tm_image(AdjArgs<T> a, const T*
   double acc_e64 = 0.0, acc_s64 = 0.0;
   auto term = [&](T lv, T eo, T sec) {
     T rhs = sec;
-    if (EONLY) rhs = cbv != T(0) ? (sec - aeff * eo) / cbv : T(0);
+    if (EONLY) rhs = cbv != T(0) ? div_fixed(sec - aeff * eo, dcb) : T(0);
     const T lamx = (eo == T(0) && rhs == T(0)) ? T(0) : lv;
     const T gca = dez ? lamx * eo * wgt : T(0);
     const T gcb = lamx * rhs * wgt;

@@ -102,6 +102,7 @@ SCALAR_SYMBOLS: Dict[str, Tuple[Tuple[str, ...], Optional[str]]] = {
     "dgb_clear_stream": ((), None),
     "dgb_set_options": (("int", "int", "int", "int"), "int"),
     "dgb_history_bytes": (("int", "int", "int", "int", "long long", "int", "int", "int", "int"), "long long"),
+    "dgb_check_fixed_division": (("float", "void*", "void*"), "int"),
     "dgb_profile": (("int",), None),
     "dgb_launch_count": ((), "long long"),
     "dgb_profile_read": (("void*", "void*", "int"), "int"),
@@ -129,6 +130,17 @@ def profile_read() -> Dict[str, Tuple[float, int]]:
     lib.dgb_profile_read(ctypes.cast(ms, ctypes.c_void_p), ctypes.cast(cnt, ctypes.c_void_p), n)
     return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(KERNEL_KINDS)}
 
+def check_fixed_division(divisor: float) -> Tuple[int, int]:
+    """(mismatches, lowest mismatching bit pattern) of the solver's division by
+    ``divisor`` against the division operator over all 2^32 float dividends."""
+    lib = load_library()
+    bad = ctypes.c_ulonglong(0)
+    first = ctypes.c_uint(0)
+    if lib.dgb_check_fixed_division(float(divisor), ctypes.addressof(bad), ctypes.addressof(first)) != 0:
+        raise NativeLibraryError(last_error(lib) or "dgb_check_fixed_division failed")
+    return int(bad.value), int(first.value)
+
+
 SOLVER_SYMBOLS = {
     "forward": (FORWARD_SIGNATURE, "float"),
     "backward": (BACKWARD_SIGNATURE, "float"),
@@ -139,6 +151,7 @@ SOLVER_SYMBOLS = {
 
 _CT = {
     "int": ctypes.c_int,
+    "float": ctypes.c_float,
     "long long": ctypes.c_longlong,
     "void*": ctypes.c_void_p,
     "char*": ctypes.c_char_p,

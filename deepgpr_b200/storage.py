@@ -32,7 +32,7 @@ from .config import (
     STORAGE_FP8_E4M3,
 )
 
-TILE_Z, TILE_Y, TILE_2D = 32, 8, 32
+TILE_Z, TILE_Y, TILE_2D = 32, 1, 32
 
 DTYPE_ALIASES = {
     "float32": torch.float32, "fp32": torch.float32, "float": torch.float32,

@@ -174,6 +174,16 @@ void dgb_forward_noalloc(
     const int* source_location, const float* source_waveform, int source_component,
     int sampling_interval, int fwi_mode, int storage_type, int save_model_history, int use_async_offload);
 
+/* Diagnostic, no counterpart in the reference.  The single-precision
+ * kernels divide by a grid spacing, by dt and by per-cell coefficients
+ * through an FMA path (Markstein's correction from the correctly rounded
+ * reciprocal) that is meant to round exactly like the division operator.
+ * This runs that path and the operator for one divisor over all 2^32 float
+ * dividends on the current device and reports the number of results whose
+ * bits differ and the lowest such dividend bit pattern (0xffffffff if none).
+ * Synchronous; returns 0, or -1 with deepgpr_last_error() set. */
+int dgb_check_fixed_division(float divisor, unsigned long long* mismatches, unsigned* first_bad);
+
 /* Process-wide kernel timing (CUDA events around every time-step
  * kernel; graph replay is off while enabled).  dgb_profile(1) clears the
  * totals; dgb_profile_read fills ms[k] and launches[k] for the kinds

@@ -56,6 +56,17 @@ def test_3d_forward_adjoint(order, cuda_device, oracle_lib):
     _compare(got, ref, grads=("grad_eps", "grad_sigma", "grad_source"))
 
 
+def test_3d_cpml_faces_of_an_axis_close_together(cuda_device, oracle_lib):
+    """x and z extents below the two face thicknesses + 4: the general per-face CPML form."""
+    p = problem_3d(nt=30, order=4, shape=(6, 14, 7), pml=3, want_source=True)
+    p.source_location = torch.tensor([[[3, 7, 3]], [[2, 5, 4]]], dtype=torch.int32)
+    p.receiver_location = torch.tensor([[[1, 3, 2], [4, 10, 5], [3, 7, 3]], [[5, 2, 6], [0, 0, 0], [2, 12, 1]]],
+                                       dtype=torch.int32)
+    ref = driver.run(p, "oracle")
+    got = run_product(p, cuda_device)
+    _compare(got, ref, grads=("grad_eps", "grad_sigma", "grad_source"))
+
+
 def test_3d_anisotropic_spacing_and_mu(cuda_device, oracle_lib):
     p = problem_3d(nt=30, order=4, pml=3, dx=(0.02, 0.017, 0.013), dt=1.0e-11)
     p.mu_r = 1.0 + 0.1 * torch.rand(p.eps_r.shape, generator=torch.Generator().manual_seed(3))
@@ -180,3 +191,12 @@ def test_2d_wide_grid_fp8(cuda_device, oracle_lib):
     got = run_product(p, cuda_device, wavefield_compression="fp8")
     assert rel_l2(got["receivers"], ref["receivers"]) <= RX_TOL
     assert rel_l2(got["grad_eps"], ref["grad_eps"]) < 5e-2
+
+
+@pytest.mark.parametrize("divisor", [0.02, 0.015, 0.017, 0.013, 0.01, 1.0, 3.0, 0.1, 7.3e-3, 2.99e-11, 1.7e-11, 0.6931, 1e6])
+def test_fixed_divisor_division_rounds_like_the_operator(divisor, cuda_device):
+    """Every float dividend (2^32 bit patterns) divides bit for bit like ``a / b``."""
+    from deepgpr_b200 import native
+
+    bad, first = native.check_fixed_division(divisor)
+    assert bad == 0, (divisor, bad, hex(first))
