@@ -285,7 +285,7 @@ constexpr int kStageSlots = 7;
 // 3D H half step (+ E^n history).  EQ: dx == dy == dz (curl scale 1).
 // ---------------------------------------------------------------------------
 template <typename T, int R, bool EQ>
-__global__ void __launch_bounds__(32 * K3_WARPS, R >= 4 ? 2 : 3) k3v_fwd_h(TiledFwd<T> P, K3Buf<T> f, K3Geom kg) {
+__global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 : 3) k3v_fwd_h(TiledFwd<T> P, K3Buf<T> f, K3Geom kg) {
   constexpr int ZLO = -(R - 1), ZHI = R + 1, NZN = ZHI - ZLO + 1;   // z neighbours of the pair, dfwd
   const FwdArgs<T>& a = P.a;
   const Grid& g = a.g;
@@ -499,8 +499,8 @@ __global__ void __launch_bounds__(32 * K3_WARPS, R >= 4 ? 2 : 3) k3v_fwd_h(Tiled
       dEy_dz[e] = dfwd_t<T, R>(fzy, tz[e]);
       dEx_dz[e] = dfwd_t<T, R>(fzx, tz[e]);
       const T cx = c1[e];
-      cyv[e] = EQ ? cx : div_fixed(cx * a.dx, a.ddy);
-      czv[e] = EQ ? cx : div_fixed(cx * a.dx, a.ddz);
+      cyv[e] = (EQ || a.dy_eq) ? cx : div_fixed(cx * a.dx, a.ddy);   // per-axis scale, as curl_scale
+      czv[e] = (EQ || a.dz_eq) ? cx : div_fixed(cx * a.dx, a.ddz);
       if (hxx && hxy && hxz[e]) hx[e] = hx[e] - cyv[e] * dEz_dy[e] + czv[e] * dEy_dz[e];
       if (hyx && hyy && hxz[e]) hy[e] = hy[e] - czv[e] * dEx_dz[e] + cx * dEz_dx[e];
       if (hyx && hxy && hzz[e]) hz[e] = hz[e] - cx * dEy_dx[e] + cyv[e] * dEx_dy[e];
@@ -637,7 +637,7 @@ __global__ void __launch_bounds__(32 * K3_WARPS, R >= 4 ? 2 : 3) k3v_fwd_h(Tiled
 // 3D E half step (+ sources, R^n history, receivers).
 // ---------------------------------------------------------------------------
 template <typename T, int R, bool EQ>
-__global__ void __launch_bounds__(32 * K3_WARPS, R >= 4 ? 2 : 3) k3v_fwd_e(TiledFwd<T> P, K3Buf<T> f, K3Geom kg) {
+__global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 : 3) k3v_fwd_e(TiledFwd<T> P, K3Buf<T> f, K3Geom kg) {
   constexpr int ZLO = -R, ZHI = R, NZN = ZHI - ZLO + 1;   // z neighbours of the pair, dback
   const FwdArgs<T>& a = P.a;
   const Grid& g = a.g;
@@ -825,8 +825,8 @@ __global__ void __launch_bounds__(32 * K3_WARPS, R >= 4 ? 2 : 3) k3v_fwd_e(Tiled
       dey[e] = degy && eyx && eyy && exz[e];
       dez[e] = degz && eyx && exy && ezz[e];
       const T cx = c1[e];
-      const T cy = EQ ? cx : div_fixed(cx * a.dx, a.ddy);
-      const T cz = EQ ? cx : div_fixed(cx * a.dx, a.ddz);
+      const T cy = (EQ || a.dy_eq) ? cx : div_fixed(cx * a.dx, a.ddy);
+      const T cz = (EQ || a.dz_eq) ? cx : div_fixed(cx * a.dx, a.ddz);
       ox[e] = ex[e];
       oy[e] = ey[e];
       oz[e] = ez[e];

@@ -1,0 +1,1076 @@
+// fdtd_3d_adj.cuh -- 3D adjoint kernels on the z-pitched working copy.
+//
+// Same decomposition as the 3D forward kernels (fdtd_3d.cuh): a warp owns
+// 64 z columns (two per lane) of one (shot, y row) and streams x planes; a
+// CTA holds four rows.  One reverse step is
+//   k3v_adj_e: lambda_H += curl^T of the E channels, then the H-CPML
+//              adjoint weights of the step at the cell;
+//   k3v_adj_h: lambda_E <- ce_hist lambda_E + curl^T of the H channels, then
+//              the head of the next reverse step at the cell (receiver
+//              cotangents, staged source terms, E-CPML adjoint weights).
+// The arithmetic of every value is that of fdtd_adjoint.cuh, which follows
+// the reference (src/DeepGPR/lib/deepgpr_cpu.c:1112-1459, 1479-1534): a
+// channel weight W of a source cell is its CPML weight(s) plus the interior
+// term; a target gathers the transposed difference of W along each axis in
+// the reference order.  Channels along x come from a register queue (the
+// entering plane's weights are formed once), along y from direct loads of
+// the neighbouring rows, along z from constant-distance shuffles plus halo
+// lanes.  Near the axis ends the gathers use per-target tap tables (zero
+// where the source point is outside the axis or its clamped stencil does not
+// reach the target), so the same code covers the whole grid.
+//
+// CPML operands of the next plane (E-face weights of the entering x plane and
+// of the lane's z columns, psi cotangents and the rhs coefficient of the
+// cell) are staged into shared memory with cp.async while the current plane
+// is computed (the forward kernels' scheme); y-face weights of neighbour rows
+// are loaded where they are used.
+#pragma once
+
+#include "fdtd_3d.cuh"
+#include "fdtd_tiled_adj.cuh"
+
+namespace dg {
+
+// Gather taps at target c of an axis of n points.  gather_back: up[r-1]
+// multiplies W(-(r-1)), dn[r-1] multiplies W(r); gather_fwd: up[r-1]
+// multiplies W(-r), dn[r-1] multiplies W(r-1) (deepgpr_cpu.c:429-507).
+template <typename T, int R>
+__device__ __forceinline__ void gtaps_back(int c, int n, T (&up)[R], T (&dn)[R]) {
+#pragma unroll
+  for (int r = 1; r <= R; ++r) {
+    const int u = c - (r - 1), d = c + r;
+    const int ru = u >= 0 ? rad_back(u, n, R) : 0, rd = d < n ? rad_back(d, n, R) : 0;
+    up[r - 1] = r <= ru ? tap<T>(ru, r) : T(0);
+    dn[r - 1] = r <= rd ? tap<T>(rd, r) : T(0);
+  }
+}
+template <typename T, int R>
+__device__ __forceinline__ void gtaps_fwd(int c, int n, T (&up)[R], T (&dn)[R]) {
+#pragma unroll
+  for (int r = 1; r <= R; ++r) {
+    const int u = c - r, d = c + r - 1;
+    const int ru = u >= 0 ? rad_fwd(u, n, R) : 0, rd = d < n ? rad_fwd(d, n, R) : 0;
+    up[r - 1] = r <= ru ? tap<T>(ru, r) : T(0);
+    dn[r - 1] = r <= rd ? tap<T>(rd, r) : T(0);
+  }
+}
+// x taps of a plane: the constant full-stencil taps away from the ends
+template <typename T, int R, bool BACK>
+__device__ __forceinline__ void xtaps(int i, int n, T (&up)[R], T (&dn)[R]) {
+  const bool full = BACK ? (i >= 2 * R - 1 && i + 2 * R - 1 < n) : (i >= 2 * R - 1 && i + 2 * R <= n);
+  if (full) {
+#pragma unroll
+    for (int r = 1; r <= R; ++r) up[r - 1] = dn[r - 1] = tap<T>(R, r);
+  } else if (BACK) {
+    gtaps_back<T, R>(i, n, up, dn);
+  } else {
+    gtaps_fwd<T, R>(i, n, up, dn);
+  }
+}
+template <typename T, int R, typename WF>
+__device__ __forceinline__ T gback_t(const WF& W, const T (&up)[R], const T (&dn)[R]) {
+  if (R == 1) {
+    T acc = W(0);
+    acc -= dn[0] * W(1);
+    return acc;
+  }
+  T acc = T(0);
+#pragma unroll
+  for (int r = 1; r <= R; ++r) {
+    acc += up[r - 1] * W(-(r - 1));
+    acc -= dn[r - 1] * W(r);
+  }
+  return acc;
+}
+template <typename T, int R, typename WF>
+__device__ __forceinline__ T gfwd_t(const WF& W, const T (&up)[R], const T (&dn)[R]) {
+  T acc = T(0);
+#pragma unroll
+  for (int r = 1; r <= R; ++r) {
+    acc += up[r - 1] * W(-r);
+    acc -= dn[r - 1] * W(r - 1);
+  }
+  return acc;
+}
+
+// Face q of coordinate c on the low / high face of an axis (E faces skip c == 0).
+template <bool EFACE>
+__device__ __forceinline__ void face_q(int plo, int phi, int c, int n, int& q0, int& q1) {
+  q0 = EFACE ? (c > 0 ? q_low_e(plo, c) : -1) : q_low_h(plo, c);
+  q1 = (EFACE && c == 0) ? -1 : q_high(phi, c, n);
+}
+
+// Element offset of a CPML array entry (psi / weight shapes of psi_dims_e/h).
+template <bool EFACE>
+__device__ __forceinline__ long long cpml_at(const Grid& g, int axis, int slot, int p, int s, int q, int i, int j,
+                                             int k) {
+  const PsiDims d = EFACE ? psi_dims_e(g, axis, slot, p) : psi_dims_h(g, axis, slot, p);
+  return psi_index(d, axis, s, q, i, j, k);
+}
+
+// Adjoint CPML weight with psi already loaded: returns w, stores psi
+// (pml_weight of fdtd_adjoint.cuh).
+template <typename T>
+__device__ __forceinline__ T pml_weight_v(T lam, T inv_h, T up, T sign, const Prof<T>& pr, T ph, T* psi) {
+  const T w = (sign * up * pr.ra1 * lam - pr.rf * ph) * inv_h;
+  *psi = sign * up * pr.rb * lam + pr.re * ph;
+  return w;
+}
+
+// curl scale along y / z (scaled() of fdtd_adjoint.cuh); EQ: dy == dz == dx
+template <bool EQ, typename T>
+__device__ __forceinline__ T curl_y(const AdjArgs<T>& a, T c) {
+  return (EQ || a.dy_eq) ? c : div_fixed(c * a.dx, a.ddy);
+}
+template <bool EQ, typename T>
+__device__ __forceinline__ T curl_z(const AdjArgs<T>& a, T c) {
+  return (EQ || a.dz_eq) ? c : div_fixed(c * a.dx, a.ddz);
+}
+
+// stage slots of the adjoint kernels
+constexpr int kAdjSlots = 13;
+enum : int {
+  kStXw1 = 0, kStXw2 = 1,      // weights of the entering x plane's channels
+  kStZw1 = 2, kStZw2 = 3,      // z-face weights of the lane's columns
+  kStPx1 = 4, kStPx2 = 5,      // psi cotangents of the cell, x face
+  kStPy1 = 6, kStPy2 = 7,      //   y face
+  kStPz1 = 8, kStPz2 = 9,      //   z face
+  kStUp = 10,                  // rhs coefficient of the cell
+  kStHw1 = 11, kStHw2 = 12     // z-face weights of the halo column (cell 0)
+};
+// dynamic shared memory of k3v_adj_e / k3v_adj_h: two stages per warp
+template <typename T>
+constexpr int k3_adj_smem_bytes() {
+  return K3_WARPS * 2 * kAdjSlots * 2 * 32 * (int)sizeof(T);
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint E step.  Channels (source = E cell), deepgpr_cpu.c:1236-1270:
+//   A_X = x faces w1 + (-c) lambda_ey,  A_Y = y faces w1 + c_y lambda_ex  -> lambda_hz
+//   B_X = x faces w2 + c lambda_ez,     B_Z = z faces w1 + (-c_z) lambda_ex -> lambda_hy
+//   C_Y = y faces w2 + (-c_y) lambda_ez, C_Z = z faces w2 + c_z lambda_ey  -> lambda_hx
+// then the H-CPML weights of step it at the cell (deepgpr_cpu.c:1331-1396).
+// ---------------------------------------------------------------------------
+template <typename T, int R, bool EQ>
+__global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 : 3)
+    k3v_adj_e(TiledAdj<T> P, K3Buf<T> f, K3Geom kg) {
+  constexpr int ZLO = -(R - 1), ZHI = R + 1, NZN = ZHI - ZLO + 1;   // z sources of the pair, gather_back
+  const AdjArgs<T>& a = P.a;
+  const Grid& g = a.g;
+  const int it = a.ctrl->cur - a.k_in_chunk;
+  if (a.want_src && blockIdx.x == 0 && threadIdx.y == 0) {
+    // waveform gradient of step it: shots summed in order (deepgpr_cpu.c:1524-1533)
+    for (int m = threadIdx.x; m < a.nsrc; m += 32) {
+      T acc = a.grad_source[(long long)m * a.nt + it];
+      for (int s = 0; s < g.nshot; ++s) acc += a.srcv[(long long)s * a.nsrc + m];
+      a.grad_source[(long long)m * a.nt + it] = acc;
+    }
+  }
+  const K3Pos wp = k3_pos(kg, g);
+  if (!wp.live) return;
+  const int NX = g.NX, NY = g.NY, NZ = g.NZ, zp = kg.zp, lane = wp.lane, s = wp.s, j = wp.j, kk = wp.kk;
+  const int PS = NY * zp;
+  const long long sbase = (long long)s * NX * PS;
+  const T* __restrict__ lEx = f.Ex + sbase;
+  const T* __restrict__ lEy = f.Ey + sbase;
+  const T* __restrict__ lEz = f.Ez + sbase;
+  T* __restrict__ lHx = f.Hx + sbase;
+  T* __restrict__ lHy = f.Hy + sbase;
+  T* __restrict__ lHz = f.Hz + sbase;
+  const T* __restrict__ cc = f.ce_curl;
+  const int hk = k3_halo<R>(wp.k0, lane);
+  const bool hok = lane < 2 * R && hk >= 0 && hk < NZ;
+  const int row = j * zp + kk;
+  const int hrow = j * zp + (hok ? hk : 0);
+  const bool pml = a.has_cpml != 0, cps = pml && kg.cpml_single;
+  // parts of the interior predicates (upd_e*): mid = 0 < c < n-1, lo = c < n-1
+  const bool dxo = NY - 1 != 1 || NZ - 1 != 1, dyo = NX - 1 != 1 || NZ - 1 != 1, dzo = NX - 1 != 1 || NY - 1 != 1;
+  const bool jm = j > 0 && j < NY - 1, jl = j < NY - 1;
+  bool kv[2], km[2], kl[2];
+  int kof[2];
+#pragma unroll
+  for (int e = 0; e < 2; ++e) {
+    const int k = kk + e;
+    kof[e] = k;
+    kv[e] = k < NZ;
+    km[e] = k > 0 && k < NZ - 1;
+    kl[e] = k < NZ - 1;
+  }
+  const bool hkm = hok && hk > 0 && hk < NZ - 1;
+  T zup[2][R], zdn[2][R], yup[R], ydn[R];
+  gtaps_back<T, R>(kk, NZ, zup[0], zdn[0]);
+  gtaps_back<T, R>(kk + 1, NZ, zup[1], zdn[1]);
+  gtaps_back<T, R>(j, NY, yup, ydn);
+  // CPML positions fixed for the warp / lane: E y faces of the neighbour rows
+  // (bit d + R - 1), E z face of the lane's columns and of its halo column,
+  // H y face of the row, H z face of the lane's columns.  With the faces of
+  // an axis apart (cps), both columns of a lane lie in the same face or none.
+  unsigned ymask = 0;
+  if (pml) {
+#pragma unroll
+    for (int d = -(R - 1); d <= R; ++d) {
+      const int y = j + d;
+      int q0, q1;
+      face_q<true>(a.eF[2].p, a.eF[3].p, y, NY, q0, q1);
+      if (y >= 0 && y < NY && (q0 >= 0 || q1 >= 0)) ymask |= 1u << (d + R - 1);
+    }
+  }
+  int ezq[2], hzq[2], ehq = -1, qhy0 = -1, qhy1 = -1;
+  bool ezlo = false, hzlo = false;   // the lane's z faces are the low ones
+#pragma unroll
+  for (int e = 0; e < 2; ++e) {
+    int q0, q1;
+    face_q<true>(a.eF[4].p, a.eF[5].p, kk + e, NZ, q0, q1);
+    ezq[e] = (cps && kv[e]) ? (q0 >= 0 ? q0 : q1) : -1;
+    ezlo |= q0 >= 0;
+    face_q<false>(a.hF[4].p, a.hF[5].p, kk + e, NZ, q0, q1);
+    hzq[e] = (cps && kv[e]) ? (q0 >= 0 ? q0 : q1) : -1;
+    hzlo |= q0 >= 0;
+  }
+  bool ehlo = true;
+  if (cps && hok) {
+    int q0, q1;
+    face_q<true>(a.eF[4].p, a.eF[5].p, hk, NZ, q0, q1);
+    ehq = q0 >= 0 ? q0 : q1;
+    ehlo = q0 >= 0;
+  }
+  if (cps) face_q<false>(a.hF[2].p, a.hF[3].p, j, NY, qhy0, qhy1);
+  const bool hy_on = qhy0 >= 0 || qhy1 >= 0;
+  const bool any_ez = __any_sync(kFullMask, ezq[0] >= 0 || ezq[1] >= 0 || ehq >= 0);
+  const bool any_hz = __any_sync(kFullMask, hzq[0] >= 0 || hzq[1] >= 0);
+
+  extern __shared__ __align__(16) unsigned char k3_adj_smem[];   // k3_adj_smem_bytes<T>()
+  T(*const sg)[kAdjSlots][2][32] = reinterpret_cast<T(*)[kAdjSlots][2][32]>(k3_adj_smem) + 2 * threadIdx.y;
+  // stages the CPML operands of plane i into stage b (one commit group per plane)
+  auto stage = [&](int i, int b) {
+    if (cps) {
+      const int xi = i + R;   // entering plane of the x channels
+      int qa, qb;
+      face_q<true>(a.eF[0].p, a.eF[1].p, xi, NX, qa, qb);
+      const bool xin = xi < NX && (qa >= 0 || qb >= 0);
+      int qh0, qh1;
+      face_q<false>(a.hF[0].p, a.hF[1].p, i, NX, qh0, qh1);
+      const bool hx_on = qh0 >= 0 || qh1 >= 0;
+      const bool il = i < NX - 1;
+      if (xin || hx_on || hy_on || any_ez || any_hz) {
+        const bool xlo = qa >= 0;
+        const int qx = xlo ? qa : qb, px = xlo ? a.eF[0].p : a.eF[1].p;
+        const T* XW1 = xlo ? a.eF[0].w1 : a.eF[1].w1;
+        const T* XW2 = xlo ? a.eF[0].w2 : a.eF[1].w2;
+        const bool hxlo = qh0 >= 0;
+        const int qhx = hxlo ? qh0 : qh1, phx = hxlo ? a.hF[0].p : a.hF[1].p;
+        const bool hylo = qhy0 >= 0;
+        const int qhy = hylo ? qhy0 : qhy1, phy = hylo ? a.hF[2].p : a.hF[3].p;
+        const int pez = ezlo ? a.eF[4].p : a.eF[5].p, phz = hzlo ? a.hF[4].p : a.hF[5].p;
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int k = kof[e];
+          if (xin && jl && kv[e]) cp_async(&sg[b][kStXw1][e][lane], XW1 + cpml_at<true>(g, 0, 1, px, s, qx, xi, j, k));
+          if (xin && kl[e]) cp_async(&sg[b][kStXw2][e][lane], XW2 + cpml_at<true>(g, 0, 2, px, s, qx, xi, j, k));
+          if (ezq[e] >= 0) {
+            if (il)
+              cp_async(&sg[b][kStZw1][e][lane],
+                       (ezlo ? a.eF[4].w1 : a.eF[5].w1) + cpml_at<true>(g, 2, 1, pez, s, ezq[e], i, j, k));
+            if (jl)
+              cp_async(&sg[b][kStZw2][e][lane],
+                       (ezlo ? a.eF[4].w2 : a.eF[5].w2) + cpml_at<true>(g, 2, 2, pez, s, ezq[e], i, j, k));
+          }
+          const bool hz_on = hzq[e] >= 0;
+          if (kv[e] && (hx_on || hy_on || hz_on)) cp_async(&sg[b][kStUp][e][lane], f.ch_rhs + i * PS + row + e);
+          if (hx_on) {
+            T* P1 = hxlo ? a.hF[0].psi1 : a.hF[1].psi1;
+            T* P2 = hxlo ? a.hF[0].psi2 : a.hF[1].psi2;
+            if (kl[e]) cp_async(&sg[b][kStPx1][e][lane], P1 + cpml_at<false>(g, 0, 1, phx, s, qhx, i, j, k));
+            if (kv[e] && jl) cp_async(&sg[b][kStPx2][e][lane], P2 + cpml_at<false>(g, 0, 2, phx, s, qhx, i, j, k));
+          }
+          if (hy_on) {
+            T* P1 = hylo ? a.hF[2].psi1 : a.hF[3].psi1;
+            T* P2 = hylo ? a.hF[2].psi2 : a.hF[3].psi2;
+            if (kl[e]) cp_async(&sg[b][kStPy1][e][lane], P1 + cpml_at<false>(g, 1, 1, phy, s, qhy, i, j, k));
+            if (kv[e] && il) cp_async(&sg[b][kStPy2][e][lane], P2 + cpml_at<false>(g, 1, 2, phy, s, qhy, i, j, k));
+          }
+          if (hz_on) {
+            T* P1 = hzlo ? a.hF[4].psi1 : a.hF[5].psi1;
+            T* P2 = hzlo ? a.hF[4].psi2 : a.hF[5].psi2;
+            if (jl) cp_async(&sg[b][kStPz1][e][lane], P1 + cpml_at<false>(g, 2, 1, phz, s, hzq[e], i, j, k));
+            if (il) cp_async(&sg[b][kStPz2][e][lane], P2 + cpml_at<false>(g, 2, 2, phz, s, hzq[e], i, j, k));
+          }
+        }
+        if (ehq >= 0) {
+          const int pe = ehlo ? a.eF[4].p : a.eF[5].p;
+          if (il)
+            cp_async(&sg[b][kStHw1][0][lane],
+                     (ehlo ? a.eF[4].w1 : a.eF[5].w1) + cpml_at<true>(g, 2, 1, pe, s, ehq, i, j, hk));
+          if (jl)
+            cp_async(&sg[b][kStHw2][0][lane],
+                     (ehlo ? a.eF[4].w2 : a.eF[5].w2) + cpml_at<true>(g, 2, 2, pe, s, ehq, i, j, hk));
+        }
+      }
+    }
+    cp_async_commit();
+  };
+
+  // x channels of plane x from its lambda_ey, lambda_ez, c (and the staged
+  // weights when the plane has an E x face)
+  auto xchan = [&](int x, const T (&ly)[2], const T (&lz)[2], const T (&c)[2], int b, T (&A)[2], T (&B)[2]) {
+    const bool xm = x > 0 && x < NX - 1;
+    int qa = -1, qb = -1;
+    if (pml) face_q<true>(a.eF[0].p, a.eF[1].p, x, NX, qa, qb);
+    const bool xin = x >= 0 && x < NX && (qa >= 0 || qb >= 0);
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      T wa = T(0), wb = T(0);
+      if (xin) {
+        if (cps) {
+          if (jl && kv[e]) wa += sg[b][kStXw1][e][lane];
+          if (kl[e]) wb += sg[b][kStXw2][e][lane];
+        } else {
+          if (jl && kv[e]) add_pml<T, true>(wa, a.eF[0], a.eF[1], g, 0, 1, s, x, j, kof[e]);
+          if (kl[e]) add_pml<T, true>(wb, a.eF[0], a.eF[1], g, 0, 2, s, x, j, kof[e]);
+        }
+      }
+      if (dyo && xm && jl && km[e]) wa += (-c[e]) * ly[e];
+      if (dzo && xm && jm && kl[e]) wb += c[e] * lz[e];
+      A[e] = wa;
+      B[e] = wb;
+    }
+  };
+
+  const int x0 = wp.x0;
+  T qA[2 * R][2], qB[2 * R][2];   // A_X, B_X at planes i-R+1 .. i+R
+#pragma unroll
+  for (int m = 0; m < 2 * R - 1; ++m) {
+    const int pl = x0 - R + 1 + m;
+    T ly[2] = {T(0), T(0)}, lz[2] = {T(0), T(0)}, c[2] = {T(0), T(0)};
+    if (pl >= 0 && pl < NX) {
+      ld2(lEy + pl * PS + row, ly);
+      ld2(lEz + pl * PS + row, lz);
+      ld2(cc + pl * PS + row, c);
+    }
+    // staged weights are not available for these planes: general form
+    const bool xm = pl > 0 && pl < NX - 1;
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      T wa = T(0), wb = T(0);
+      if (pml && pl >= 0 && pl < NX) {
+        if (jl && kv[e]) add_pml<T, true>(wa, a.eF[0], a.eF[1], g, 0, 1, s, pl, j, kof[e]);
+        if (kl[e]) add_pml<T, true>(wb, a.eF[0], a.eF[1], g, 0, 2, s, pl, j, kof[e]);
+      }
+      if (dyo && xm && jl && km[e]) wa += (-c[e]) * ly[e];
+      if (dzo && xm && jm && kl[e]) wb += c[e] * lz[e];
+      qA[m][e] = wa;
+      qB[m][e] = wb;
+    }
+  }
+  // operands of the next plane
+  T nyR[2], nzR[2], ncR[2];           // plane i+R: lambda_ey, lambda_ez, c
+  T nx[2], ny[2], nz[2], nc[2];       // plane i: lambda_ex, lambda_ey, lambda_ez, c
+  T nhx[2], nhy[2], nhz[2];           // plane i: lambda_H
+  T nhex = T(0), nhey = T(0), nhc = T(0);   // halo column: lambda_ex, lambda_ey, c
+  auto fetch = [&](int i) {
+    const int o = i * PS;
+    if (i + R < NX) {
+      ld2(lEy + o + R * PS + row, nyR);
+      ld2(lEz + o + R * PS + row, nzR);
+      ld2(cc + o + R * PS + row, ncR);
+    } else {
+      nyR[0] = nyR[1] = nzR[0] = nzR[1] = ncR[0] = ncR[1] = T(0);
+    }
+    ld2(lEx + o + row, nx);
+    ld2(lEy + o + row, ny);
+    ld2(lEz + o + row, nz);
+    ld2(cc + o + row, nc);
+    ld2(lHx + o + row, nhx);
+    ld2(lHy + o + row, nhy);
+    ld2(lHz + o + row, nhz);
+    if (hok) {
+      nhex = lEx[o + hrow];
+      nhey = lEy[o + hrow];
+      nhc = cc[o + hrow];
+    }
+  };
+  fetch(x0);
+  stage(x0, 0);
+  for (int i = x0; i < wp.x1; ++i) {
+    T yR[2], zR[2], cR[2], ex[2], ey[2], ez[2], c[2], hx[2], hy[2], hz[2];
+    const T hex = nhex, hey = nhey, hc = nhc;
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      yR[e] = nyR[e];
+      zR[e] = nzR[e];
+      cR[e] = ncR[e];
+      ex[e] = nx[e];
+      ey[e] = ny[e];
+      ez[e] = nz[e];
+      c[e] = nc[e];
+      hx[e] = nhx[e];
+      hy[e] = nhy[e];
+      hz[e] = nhz[e];
+    }
+    if (i + 1 < wp.x1) {
+      fetch(i + 1);
+      stage(i + 1, (i + 1 - x0) & 1);
+    } else {
+      cp_async_commit();
+    }
+    cp_async_wait_prev();
+    const int b = (i - x0) & 1;
+    const int o = i * PS;
+    const bool il = i < NX - 1, im = i > 0 && i < NX - 1;
+    xchan(i + R, yR, zR, cR, b, qA[2 * R - 1], qB[2 * R - 1]);
+    // z channels of the lane's columns and of the halo column
+    T bz[2], cz[2], hbz = T(0), hcz = T(0);
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      T w1 = T(0), w2 = T(0);
+      if (cps) {
+        if (ezq[e] >= 0 && il) w1 += sg[b][kStZw1][e][lane];
+        if (ezq[e] >= 0 && jl) w2 += sg[b][kStZw2][e][lane];
+      } else if (pml && kv[e]) {
+        if (il) add_pml<T, true>(w1, a.eF[4], a.eF[5], g, 2, 1, s, i, j, kof[e]);
+        if (jl) add_pml<T, true>(w2, a.eF[4], a.eF[5], g, 2, 2, s, i, j, kof[e]);
+      }
+      const T cze = curl_z<EQ>(a, c[e]);
+      if (dxo && il && jm && km[e]) w1 += (-cze) * ex[e];
+      if (dyo && im && jl && km[e]) w2 += cze * ey[e];
+      bz[e] = w1;
+      cz[e] = w2;
+    }
+    if (hok) {
+      if (cps) {
+        if (ehq >= 0 && il) hbz += sg[b][kStHw1][0][lane];
+        if (ehq >= 0 && jl) hcz += sg[b][kStHw2][0][lane];
+      } else if (pml) {
+        if (il) add_pml<T, true>(hbz, a.eF[4], a.eF[5], g, 2, 1, s, i, j, hk);
+        if (jl) add_pml<T, true>(hcz, a.eF[4], a.eF[5], g, 2, 2, s, i, j, hk);
+      }
+      const T czh = curl_z<EQ>(a, hc);
+      if (dxo && il && jm && hkm) hbz += (-czh) * hex;
+      if (dyo && im && jl && hkm) hcz += czh * hey;
+    }
+    T zb[NZN], zc[NZN];
+    znb<T, R, ZLO, ZHI>(bz, hbz, lane, zb);
+    znb<T, R, ZLO, ZHI>(cz, hcz, lane, zc);
+    // y channels of rows j + d (own row from the registers)
+    T ay[2 * R][2], cy[2 * R][2];
+#pragma unroll
+    for (int d = -(R - 1); d <= R; ++d) {
+      const int y = j + d;
+      const int m = d + R - 1;
+      T lx[2], lz[2], cv[2];
+      if (d == 0) {
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          lx[e] = ex[e];
+          lz[e] = ez[e];
+          cv[e] = c[e];
+        }
+      } else if (y >= 0 && y < NY) {
+        ld2(lEx + o + row + d * zp, lx);
+        ld2(lEz + o + row + d * zp, lz);
+        ld2(cc + o + row + d * zp, cv);
+      } else {
+        lx[0] = lx[1] = lz[0] = lz[1] = cv[0] = cv[1] = T(0);
+      }
+      const bool ym = y > 0 && y < NY - 1;
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        T w1 = T(0), w2 = T(0);
+        if ((ymask >> m) & 1u) {
+          if (il && kv[e]) add_pml<T, true>(w1, a.eF[2], a.eF[3], g, 1, 1, s, i, y, kof[e]);
+          if (kl[e]) add_pml<T, true>(w2, a.eF[2], a.eF[3], g, 1, 2, s, i, y, kof[e]);
+        }
+        const T cye = curl_y<EQ>(a, cv[e]);
+        if (dxo && il && ym && km[e]) w1 += cye * lx[e];
+        if (dzo && im && ym && kl[e]) w2 += (-cye) * lz[e];
+        ay[m][e] = w1;
+        cy[m][e] = w2;
+      }
+    }
+    // gathers, in the reference order
+    T xup[R], xdn[R];
+    xtaps<T, R, true>(i, NX, xup, xdn);
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      hz[e] += gback_t<T, R>([&](int d) { return qA[R - 1 + d][e]; }, xup, xdn);
+      hz[e] += gback_t<T, R>([&](int d) { return ay[d + R - 1][e]; }, yup, ydn);
+      hy[e] += gback_t<T, R>([&](int d) { return qB[R - 1 + d][e]; }, xup, xdn);
+      hy[e] += gback_t<T, R>([&](int d) { return zb[e + d - ZLO]; }, zup[e], zdn[e]);
+      hx[e] += gback_t<T, R>([&](int d) { return cy[d + R - 1][e]; }, yup, ydn);
+      hx[e] += gback_t<T, R>([&](int d) { return zc[e + d - ZLO]; }, zup[e], zdn[e]);
+    }
+    if (kv[1]) {
+      st2(lHx + o + row, hx);
+      st2(lHy + o + row, hy);
+      st2(lHz + o + row, hz);
+    } else if (kv[0]) {
+      lHx[o + row] = hx[0];
+      lHy[o + row] = hy[0];
+      lHz[o + row] = hz[0];
+    }
+    // H-CPML adjoint weights of step it at the cell
+    if (cps) {
+      int qh0, qh1;
+      face_q<false>(a.hF[0].p, a.hF[1].p, i, NX, qh0, qh1);
+      const bool hx_on = qh0 >= 0 || qh1 >= 0;
+      if (hx_on || hy_on || any_hz) {
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const bool hz_on = hzq[e] >= 0;
+          if (!(kv[e] && (hx_on || hy_on || hz_on))) continue;
+          const T up = sg[b][kStUp][e][lane];
+          const int k = kof[e];
+          if (hx_on) {
+            const bool lo = qh0 >= 0;
+            const Face<T>& F = lo ? a.hF[0] : a.hF[1];
+            const int q = lo ? qh0 : qh1;
+            const Prof<T> pr = prof(F, q);
+            if (kl[e]) {
+              const long long pi = cpml_at<false>(g, 0, 1, F.p, s, q, i, j, k);
+              F.w1[pi] = pml_weight_v(hy[e], a.inv_dx, up, T(1), pr, sg[b][kStPx1][e][lane], &F.psi1[pi]);
+            }
+            if (jl) {
+              const long long pi = cpml_at<false>(g, 0, 2, F.p, s, q, i, j, k);
+              F.w2[pi] = pml_weight_v(hz[e], a.inv_dx, up, T(-1), pr, sg[b][kStPx2][e][lane], &F.psi2[pi]);
+            }
+          }
+          if (hy_on) {
+            const bool lo = qhy0 >= 0;
+            const Face<T>& F = lo ? a.hF[2] : a.hF[3];
+            const int q = lo ? qhy0 : qhy1;
+            const Prof<T> pr = prof(F, q);
+            if (kl[e]) {
+              const long long pi = cpml_at<false>(g, 1, 1, F.p, s, q, i, j, k);
+              F.w1[pi] = pml_weight_v(hx[e], a.inv_dy, up, T(-1), pr, sg[b][kStPy1][e][lane], &F.psi1[pi]);
+            }
+            if (il) {
+              const long long pi = cpml_at<false>(g, 1, 2, F.p, s, q, i, j, k);
+              F.w2[pi] = pml_weight_v(hz[e], a.inv_dy, up, T(1), pr, sg[b][kStPy2][e][lane], &F.psi2[pi]);
+            }
+          }
+          if (hz_on) {
+            const Face<T>& F = hzlo ? a.hF[4] : a.hF[5];
+            const int q = hzq[e];
+            const Prof<T> pr = prof(F, q);
+            if (jl) {
+              const long long pi = cpml_at<false>(g, 2, 1, F.p, s, q, i, j, k);
+              F.w1[pi] = pml_weight_v(hx[e], a.inv_dz, up, T(1), pr, sg[b][kStPz1][e][lane], &F.psi1[pi]);
+            }
+            if (il) {
+              const long long pi = cpml_at<false>(g, 2, 2, F.p, s, q, i, j, k);
+              F.w2[pi] = pml_weight_v(hy[e], a.inv_dz, up, T(-1), pr, sg[b][kStPz2][e][lane], &F.psi2[pi]);
+            }
+          }
+        }
+      }
+    } else if (pml) {
+      // faces of one axis meet: every face in turn, direct loads
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        if (!kv[e]) continue;
+        const int k = kof[e];
+        int qh[6];
+        face_q<false>(a.hF[0].p, a.hF[1].p, i, NX, qh[0], qh[1]);
+        face_q<false>(a.hF[2].p, a.hF[3].p, j, NY, qh[2], qh[3]);
+        face_q<false>(a.hF[4].p, a.hF[5].p, k, NZ, qh[4], qh[5]);
+        if (qh[0] < 0 && qh[1] < 0 && qh[2] < 0 && qh[3] < 0 && qh[4] < 0 && qh[5] < 0) continue;
+        const T up = f.ch_rhs[o + row + e];
+#pragma unroll
+        for (int fc = 0; fc < 6; ++fc) {
+          const int q = qh[fc];
+          if (q < 0) continue;
+          const Face<T>& F = a.hF[fc];
+          const Prof<T> pr = prof(F, q);
+          const int axis = fc >> 1;
+          const bool on1 = axis == 2 ? jl : kl[e];
+          const bool on2 = axis == 0 ? jl : il;
+          const T l1 = axis == 0 ? hy[e] : hx[e];
+          const T l2 = axis == 2 ? hy[e] : hz[e];
+          const T ih = axis == 0 ? a.inv_dx : (axis == 1 ? a.inv_dy : a.inv_dz);
+          const T s1 = axis == 1 ? T(-1) : T(1);
+          const T s2 = axis == 1 ? T(1) : T(-1);
+          if (on1) {
+            const long long pi = cpml_at<false>(g, axis, 1, F.p, s, q, i, j, k);
+            F.w1[pi] = pml_weight(l1, ih, up, s1, pr, &F.psi1[pi]);
+          }
+          if (on2) {
+            const long long pi = cpml_at<false>(g, axis, 2, F.p, s, q, i, j, k);
+            F.w2[pi] = pml_weight(l2, ih, up, s2, pr, &F.psi2[pi]);
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int m = 0; m < 2 * R - 1; ++m)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        qA[m][e] = qA[m + 1][e];
+        qB[m][e] = qB[m + 1][e];
+      }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint H step.  Channels (source = H cell), deepgpr_cpu.c:1400-1424:
+//   A_X = x faces w1 + c lambda_hy,      A_Y = y faces w1 + (-c_y) lambda_hx -> lambda_ez
+//   B_X = x faces w2 + (-c) lambda_hz,   B_Z = z faces w1 + c_z lambda_hx    -> lambda_ey
+//   C_Y = y faces w2 + c_y lambda_hz,    C_Z = z faces w2 + (-c_z) lambda_hy -> lambda_ex
+// then the head of step it-1 at the cell.
+// ---------------------------------------------------------------------------
+template <typename T, int R, bool EQ>
+__global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 : 3)
+    k3v_adj_h(TiledAdj<T> P, K3Buf<T> f, K3Geom kg) {
+  constexpr int ZLO = -R, ZHI = R, NZN = ZHI - ZLO + 1;   // z sources of the pair, gather_fwd
+  const AdjArgs<T>& a = P.a;
+  const Grid& g = a.g;
+  const K3Pos wp = k3_pos(kg, g);
+  if (!wp.live) return;
+  const int NX = g.NX, NY = g.NY, NZ = g.NZ, zp = kg.zp, lane = wp.lane, s = wp.s, j = wp.j, kk = wp.kk;
+  const int PS = NY * zp;
+  const long long sbase = (long long)s * NX * PS;
+  T* __restrict__ lEx = f.Ex + sbase;
+  T* __restrict__ lEy = f.Ey + sbase;
+  T* __restrict__ lEz = f.Ez + sbase;
+  const T* __restrict__ lHx = f.Hx + sbase;
+  const T* __restrict__ lHy = f.Hy + sbase;
+  const T* __restrict__ lHz = f.Hz + sbase;
+  const T* __restrict__ hcf = f.ch_curl;
+  const int it = a.ctrl->cur - a.k_in_chunk;
+  const int head = it - 1;
+  const int hk = k3_halo<R>(wp.k0, lane);
+  const bool hok = lane < 2 * R && hk >= 0 && hk < NZ;
+  const int row = j * zp + kk;
+  const int hrow = j * zp + (hok ? hk : 0);
+  const bool pml = a.has_cpml != 0, cps = pml && kg.cpml_single;
+  // parts of upd_h*: hx: NX-1 != 1, mid(i), lo(j), lo(k); hy: NY-1 != 1, lo(i),
+  // mid(j), lo(k); hz: NZ-1 != 1, lo(i), lo(j), mid(k); and of upd_e* for ce_hist
+  const bool hxo = NX - 1 != 1, hyo = NY - 1 != 1, hzo = NZ - 1 != 1;
+  const bool dxo = NY - 1 != 1 || NZ - 1 != 1, dyo = NX - 1 != 1 || NZ - 1 != 1, dzo = NX - 1 != 1 || NY - 1 != 1;
+  const bool jm = j > 0 && j < NY - 1, jl = j < NY - 1;
+  bool kv[2], km[2], kl[2];
+  int kof[2];
+#pragma unroll
+  for (int e = 0; e < 2; ++e) {
+    const int k = kk + e;
+    kof[e] = k;
+    kv[e] = k < NZ;
+    km[e] = k > 0 && k < NZ - 1;
+    kl[e] = k < NZ - 1;
+  }
+  const bool hkl = hok && hk < NZ - 1;
+  T zup[2][R], zdn[2][R], yup[R], ydn[R];
+  gtaps_fwd<T, R>(kk, NZ, zup[0], zdn[0]);
+  gtaps_fwd<T, R>(kk + 1, NZ, zup[1], zdn[1]);
+  gtaps_fwd<T, R>(j, NY, yup, ydn);
+  unsigned ymask = 0;   // H y faces of rows j + d (bit d + R)
+  if (pml) {
+#pragma unroll
+    for (int d = -R; d <= R - 1; ++d) {
+      const int y = j + d;
+      int q0, q1;
+      face_q<false>(a.hF[2].p, a.hF[3].p, y, NY, q0, q1);
+      if (y >= 0 && y < NY && (q0 >= 0 || q1 >= 0)) ymask |= 1u << (d + R);
+    }
+  }
+  int hzq[2], ezq[2], hhq = -1, qey0 = -1, qey1 = -1;
+  bool hzlo = false, ezlo = false;
+#pragma unroll
+  for (int e = 0; e < 2; ++e) {
+    int q0, q1;
+    face_q<false>(a.hF[4].p, a.hF[5].p, kk + e, NZ, q0, q1);
+    hzq[e] = (cps && kv[e]) ? (q0 >= 0 ? q0 : q1) : -1;
+    hzlo |= q0 >= 0;
+    face_q<true>(a.eF[4].p, a.eF[5].p, kk + e, NZ, q0, q1);
+    ezq[e] = (cps && kv[e]) ? (q0 >= 0 ? q0 : q1) : -1;
+    ezlo |= q0 >= 0;
+  }
+  bool hhlo = true;
+  if (cps && hok) {
+    int q0, q1;
+    face_q<false>(a.hF[4].p, a.hF[5].p, hk, NZ, q0, q1);
+    hhq = q0 >= 0 ? q0 : q1;
+    hhlo = q0 >= 0;
+  }
+  if (cps) face_q<true>(a.eF[2].p, a.eF[3].p, j, NY, qey0, qey1);
+  const bool ey_on = qey0 >= 0 || qey1 >= 0;
+  const bool any_hz = __any_sync(kFullMask, hzq[0] >= 0 || hzq[1] >= 0 || hhq >= 0);
+  const bool any_ez = __any_sync(kFullMask, ezq[0] >= 0 || ezq[1] >= 0);
+  const bool heads = head >= 0;
+
+  extern __shared__ __align__(16) unsigned char k3_adj_smem[];   // k3_adj_smem_bytes<T>()
+  T(*const sg)[kAdjSlots][2][32] = reinterpret_cast<T(*)[kAdjSlots][2][32]>(k3_adj_smem) + 2 * threadIdx.y;
+  auto stage = [&](int i, int b) {
+    if (cps) {
+      const int xi = i + R - 1;   // entering plane of the x channels
+      int qa, qb;
+      face_q<false>(a.hF[0].p, a.hF[1].p, xi, NX, qa, qb);
+      const bool xin = xi < NX && (qa >= 0 || qb >= 0);
+      int qe0 = -1, qe1 = -1;
+      if (heads) face_q<true>(a.eF[0].p, a.eF[1].p, i, NX, qe0, qe1);
+      const bool ex_on = qe0 >= 0 || qe1 >= 0;
+      const bool il = i < NX - 1;
+      if (xin || ex_on || (heads && (ey_on || any_ez)) || any_hz) {
+        const bool xlo = qa >= 0;
+        const int qx = xlo ? qa : qb, px = xlo ? a.hF[0].p : a.hF[1].p;
+        const T* XW1 = xlo ? a.hF[0].w1 : a.hF[1].w1;
+        const T* XW2 = xlo ? a.hF[0].w2 : a.hF[1].w2;
+        const bool exlo = qe0 >= 0;
+        const int qex = exlo ? qe0 : qe1, pex = exlo ? a.eF[0].p : a.eF[1].p;
+        const bool eylo = qey0 >= 0;
+        const int qey = eylo ? qey0 : qey1, pey = eylo ? a.eF[2].p : a.eF[3].p;
+        const int phz = hzlo ? a.hF[4].p : a.hF[5].p, pez = ezlo ? a.eF[4].p : a.eF[5].p;
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int k = kof[e];
+          if (xin && kl[e]) cp_async(&sg[b][kStXw1][e][lane], XW1 + cpml_at<false>(g, 0, 1, px, s, qx, xi, j, k));
+          if (xin && jl && kv[e]) cp_async(&sg[b][kStXw2][e][lane], XW2 + cpml_at<false>(g, 0, 2, px, s, qx, xi, j, k));
+          if (hzq[e] >= 0) {
+            if (jl)
+              cp_async(&sg[b][kStZw1][e][lane],
+                       (hzlo ? a.hF[4].w1 : a.hF[5].w1) + cpml_at<false>(g, 2, 1, phz, s, hzq[e], i, j, k));
+            if (il)
+              cp_async(&sg[b][kStZw2][e][lane],
+                       (hzlo ? a.hF[4].w2 : a.hF[5].w2) + cpml_at<false>(g, 2, 2, phz, s, hzq[e], i, j, k));
+          }
+          if (!heads) continue;
+          const bool ez_on = ezq[e] >= 0;
+          if (kv[e] && (ex_on || ey_on || ez_on)) cp_async(&sg[b][kStUp][e][lane], f.ce_rhs + i * PS + row + e);
+          if (ex_on) {
+            T* P1 = exlo ? a.eF[0].psi1 : a.eF[1].psi1;
+            T* P2 = exlo ? a.eF[0].psi2 : a.eF[1].psi2;
+            if (kv[e] && jl) cp_async(&sg[b][kStPx1][e][lane], P1 + cpml_at<true>(g, 0, 1, pex, s, qex, i, j, k));
+            if (kl[e]) cp_async(&sg[b][kStPx2][e][lane], P2 + cpml_at<true>(g, 0, 2, pex, s, qex, i, j, k));
+          }
+          if (ey_on) {
+            T* P1 = eylo ? a.eF[2].psi1 : a.eF[3].psi1;
+            T* P2 = eylo ? a.eF[2].psi2 : a.eF[3].psi2;
+            if (kv[e] && il) cp_async(&sg[b][kStPy1][e][lane], P1 + cpml_at<true>(g, 1, 1, pey, s, qey, i, j, k));
+            if (kl[e]) cp_async(&sg[b][kStPy2][e][lane], P2 + cpml_at<true>(g, 1, 2, pey, s, qey, i, j, k));
+          }
+          if (ez_on) {
+            T* P1 = ezlo ? a.eF[4].psi1 : a.eF[5].psi1;
+            T* P2 = ezlo ? a.eF[4].psi2 : a.eF[5].psi2;
+            if (il) cp_async(&sg[b][kStPz1][e][lane], P1 + cpml_at<true>(g, 2, 1, pez, s, ezq[e], i, j, k));
+            if (jl) cp_async(&sg[b][kStPz2][e][lane], P2 + cpml_at<true>(g, 2, 2, pez, s, ezq[e], i, j, k));
+          }
+        }
+        if (hhq >= 0) {
+          const int ph = hhlo ? a.hF[4].p : a.hF[5].p;
+          if (jl)
+            cp_async(&sg[b][kStHw1][0][lane],
+                     (hhlo ? a.hF[4].w1 : a.hF[5].w1) + cpml_at<false>(g, 2, 1, ph, s, hhq, i, j, hk));
+          if (il)
+            cp_async(&sg[b][kStHw2][0][lane],
+                     (hhlo ? a.hF[4].w2 : a.hF[5].w2) + cpml_at<false>(g, 2, 2, ph, s, hhq, i, j, hk));
+        }
+      }
+    }
+    cp_async_commit();
+  };
+
+  auto xchan = [&](int x, const T (&ly)[2], const T (&lz)[2], const T (&c)[2], int b, T (&A)[2], T (&B)[2]) {
+    const bool xl = x >= 0 && x < NX - 1;
+    int qa = -1, qb = -1;
+    if (pml) face_q<false>(a.hF[0].p, a.hF[1].p, x, NX, qa, qb);
+    const bool xin = x >= 0 && x < NX && (qa >= 0 || qb >= 0);
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      T wa = T(0), wb = T(0);
+      if (xin) {
+        if (cps) {
+          if (kl[e]) wa += sg[b][kStXw1][e][lane];
+          if (jl && kv[e]) wb += sg[b][kStXw2][e][lane];
+        } else {
+          if (kl[e]) add_pml<T, false>(wa, a.hF[0], a.hF[1], g, 0, 1, s, x, j, kof[e]);
+          if (jl && kv[e]) add_pml<T, false>(wb, a.hF[0], a.hF[1], g, 0, 2, s, x, j, kof[e]);
+        }
+      }
+      if (hyo && xl && jm && kl[e]) wa += c[e] * ly[e];
+      if (hzo && xl && jl && km[e]) wb += (-c[e]) * lz[e];
+      A[e] = wa;
+      B[e] = wb;
+    }
+  };
+
+  const int x0 = wp.x0;
+  T qA[2 * R][2], qB[2 * R][2];   // A_X, B_X at planes i-R .. i+R-1
+#pragma unroll
+  for (int m = 0; m < 2 * R - 1; ++m) {
+    const int pl = x0 - R + m;
+    T ly[2] = {T(0), T(0)}, lz[2] = {T(0), T(0)}, c[2] = {T(0), T(0)};
+    if (pl >= 0 && pl < NX) {
+      ld2(lHy + pl * PS + row, ly);
+      ld2(lHz + pl * PS + row, lz);
+      ld2(hcf + pl * PS + row, c);
+    }
+    const bool xl = pl >= 0 && pl < NX - 1;
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      T wa = T(0), wb = T(0);
+      if (pml && pl >= 0 && pl < NX) {
+        if (kl[e]) add_pml<T, false>(wa, a.hF[0], a.hF[1], g, 0, 1, s, pl, j, kof[e]);
+        if (jl && kv[e]) add_pml<T, false>(wb, a.hF[0], a.hF[1], g, 0, 2, s, pl, j, kof[e]);
+      }
+      if (hyo && xl && jm && kl[e]) wa += c[e] * ly[e];
+      if (hzo && xl && jl && km[e]) wb += (-c[e]) * lz[e];
+      qA[m][e] = wa;
+      qB[m][e] = wb;
+    }
+  }
+  T nyR[2], nzR[2], ncR[2];               // plane i+R-1: lambda_hy, lambda_hz, c
+  T nhx[2], nhy[2], nhz[2], nc[2];        // plane i: lambda_H, c
+  T nex[2], ney[2], nez[2], nca[2];       // plane i: lambda_E, ce_hist
+  T nhhx = T(0), nhhy = T(0), nhc = T(0);   // halo column: lambda_hx, lambda_hy, c
+  auto fetch = [&](int i) {
+    const int o = i * PS;
+    if (i + R - 1 < NX) {
+      ld2(lHy + o + (R - 1) * PS + row, nyR);
+      ld2(lHz + o + (R - 1) * PS + row, nzR);
+      ld2(hcf + o + (R - 1) * PS + row, ncR);
+    } else {
+      nyR[0] = nyR[1] = nzR[0] = nzR[1] = ncR[0] = ncR[1] = T(0);
+    }
+    ld2(lHx + o + row, nhx);
+    ld2(lHy + o + row, nhy);
+    ld2(lHz + o + row, nhz);
+    ld2(hcf + o + row, nc);
+    ld2(lEx + o + row, nex);
+    ld2(lEy + o + row, ney);
+    ld2(lEz + o + row, nez);
+    ld2(f.ce_hist + o + row, nca);
+    if (hok) {
+      nhhx = lHx[o + hrow];
+      nhhy = lHy[o + hrow];
+      nhc = hcf[o + hrow];
+    }
+  };
+  fetch(x0);
+  stage(x0, 0);
+  for (int i = x0; i < wp.x1; ++i) {
+    T yR[2], zR[2], cR[2], hx[2], hy[2], hz[2], c[2], ex[2], ey[2], ez[2], ca[2];
+    const T hhx = nhhx, hhy = nhhy, hc = nhc;
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      yR[e] = nyR[e];
+      zR[e] = nzR[e];
+      cR[e] = ncR[e];
+      hx[e] = nhx[e];
+      hy[e] = nhy[e];
+      hz[e] = nhz[e];
+      c[e] = nc[e];
+      ex[e] = nex[e];
+      ey[e] = ney[e];
+      ez[e] = nez[e];
+      ca[e] = nca[e];
+    }
+    if (i + 1 < wp.x1) {
+      fetch(i + 1);
+      stage(i + 1, (i + 1 - x0) & 1);
+    } else {
+      cp_async_commit();
+    }
+    cp_async_wait_prev();
+    const int b = (i - x0) & 1;
+    const int o = i * PS;
+    const bool il = i < NX - 1, im = i > 0 && i < NX - 1;
+    xchan(i + R - 1, yR, zR, cR, b, qA[2 * R - 1], qB[2 * R - 1]);
+    T bz[2], cz[2], hbz = T(0), hcz = T(0);
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      T w1 = T(0), w2 = T(0);
+      if (cps) {
+        if (hzq[e] >= 0 && jl) w1 += sg[b][kStZw1][e][lane];
+        if (hzq[e] >= 0 && il) w2 += sg[b][kStZw2][e][lane];
+      } else if (pml && kv[e]) {
+        if (jl) add_pml<T, false>(w1, a.hF[4], a.hF[5], g, 2, 1, s, i, j, kof[e]);
+        if (il) add_pml<T, false>(w2, a.hF[4], a.hF[5], g, 2, 2, s, i, j, kof[e]);
+      }
+      const T cze = curl_z<EQ>(a, c[e]);
+      if (hxo && im && jl && kl[e]) w1 += cze * hx[e];
+      if (hyo && il && jm && kl[e]) w2 += (-cze) * hy[e];
+      bz[e] = w1;
+      cz[e] = w2;
+    }
+    if (hok) {
+      if (cps) {
+        if (hhq >= 0 && jl) hbz += sg[b][kStHw1][0][lane];
+        if (hhq >= 0 && il) hcz += sg[b][kStHw2][0][lane];
+      } else if (pml) {
+        if (jl) add_pml<T, false>(hbz, a.hF[4], a.hF[5], g, 2, 1, s, i, j, hk);
+        if (il) add_pml<T, false>(hcz, a.hF[4], a.hF[5], g, 2, 2, s, i, j, hk);
+      }
+      const T czh = curl_z<EQ>(a, hc);
+      if (hxo && im && jl && hkl) hbz += czh * hhx;
+      if (hyo && il && jm && hkl) hcz += (-czh) * hhy;
+    }
+    T zb[NZN], zc[NZN];
+    znb<T, R, ZLO, ZHI>(bz, hbz, lane, zb);
+    znb<T, R, ZLO, ZHI>(cz, hcz, lane, zc);
+    T ay[2 * R][2], cy[2 * R][2];   // A_Y, C_Y at rows j + d, d = -R .. R-1
+#pragma unroll
+    for (int d = -R; d <= R - 1; ++d) {
+      const int y = j + d;
+      const int m = d + R;
+      T lx[2], lz[2], cv[2];
+      if (d == 0) {
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          lx[e] = hx[e];
+          lz[e] = hz[e];
+          cv[e] = c[e];
+        }
+      } else if (y >= 0 && y < NY) {
+        ld2(lHx + o + row + d * zp, lx);
+        ld2(lHz + o + row + d * zp, lz);
+        ld2(hcf + o + row + d * zp, cv);
+      } else {
+        lx[0] = lx[1] = lz[0] = lz[1] = cv[0] = cv[1] = T(0);
+      }
+      const bool yl = y >= 0 && y < NY - 1;
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        T w1 = T(0), w2 = T(0);
+        if ((ymask >> m) & 1u) {
+          if (kl[e]) add_pml<T, false>(w1, a.hF[2], a.hF[3], g, 1, 1, s, i, y, kof[e]);
+          if (il && kv[e]) add_pml<T, false>(w2, a.hF[2], a.hF[3], g, 1, 2, s, i, y, kof[e]);
+        }
+        const T cye = curl_y<EQ>(a, cv[e]);
+        if (hxo && im && yl && kl[e]) w1 += (-cye) * lx[e];
+        if (hzo && il && yl && km[e]) w2 += cye * lz[e];
+        ay[m][e] = w1;
+        cy[m][e] = w2;
+      }
+    }
+    T xup[R], xdn[R];
+    xtaps<T, R, false>(i, NX, xup, xdn);
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      if (dxo && il && jm && km[e]) ex[e] = ca[e] * ex[e];
+      if (dyo && im && jl && km[e]) ey[e] = ca[e] * ey[e];
+      if (dzo && im && jm && kl[e]) ez[e] = ca[e] * ez[e];
+      ez[e] += gfwd_t<T, R>([&](int d) { return qA[R + d][e]; }, xup, xdn);
+      ez[e] += gfwd_t<T, R>([&](int d) { return ay[d + R][e]; }, yup, ydn);
+      ey[e] += gfwd_t<T, R>([&](int d) { return qB[R + d][e]; }, xup, xdn);
+      ey[e] += gfwd_t<T, R>([&](int d) { return zb[e + d - ZLO]; }, zup[e], zdn[e]);
+      ex[e] += gfwd_t<T, R>([&](int d) { return cy[d + R][e]; }, yup, ydn);
+      ex[e] += gfwd_t<T, R>([&](int d) { return zc[e + d - ZLO]; }, zup[e], zdn[e]);
+    }
+    if (heads) {
+      // receiver cotangents and staged source terms of step it-1
+      const bool pts = (kg.src_rows && kg.src_rows[(long long)s * NX + i]) ||
+                       (kg.rcv_rows && kg.rcv_rows[(long long)s * NX + i]);
+      if (pts) {
+#pragma unroll
+        for (int e = 0; e < 2; ++e)
+          if (kv[e]) tiled_head(P, head, s, (i * NY + j) * NZ + kof[e], ex[e], ey[e], ez[e]);
+      }
+      // E-CPML adjoint weights of step it-1
+      if (cps) {
+        int qe0, qe1;
+        face_q<true>(a.eF[0].p, a.eF[1].p, i, NX, qe0, qe1);
+        const bool ex_on = qe0 >= 0 || qe1 >= 0;
+        if (ex_on || ey_on || any_ez) {
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            const bool ez_on = ezq[e] >= 0;
+            if (!(kv[e] && (ex_on || ey_on || ez_on))) continue;
+            const T up = sg[b][kStUp][e][lane];
+            const int k = kof[e];
+            if (ex_on) {
+              const bool lo = qe0 >= 0;
+              const Face<T>& F = lo ? a.eF[0] : a.eF[1];
+              const int q = lo ? qe0 : qe1;
+              const Prof<T> pr = prof(F, q);
+              if (jl) {
+                const long long pi = cpml_at<true>(g, 0, 1, F.p, s, q, i, j, k);
+                F.w1[pi] = pml_weight_v(ey[e], a.inv_dx, up, T(-1), pr, sg[b][kStPx1][e][lane], &F.psi1[pi]);
+              }
+              if (kl[e]) {
+                const long long pi = cpml_at<true>(g, 0, 2, F.p, s, q, i, j, k);
+                F.w2[pi] = pml_weight_v(ez[e], a.inv_dx, up, T(1), pr, sg[b][kStPx2][e][lane], &F.psi2[pi]);
+              }
+            }
+            if (ey_on) {
+              const bool lo = qey0 >= 0;
+              const Face<T>& F = lo ? a.eF[2] : a.eF[3];
+              const int q = lo ? qey0 : qey1;
+              const Prof<T> pr = prof(F, q);
+              if (il) {
+                const long long pi = cpml_at<true>(g, 1, 1, F.p, s, q, i, j, k);
+                F.w1[pi] = pml_weight_v(ex[e], a.inv_dy, up, T(1), pr, sg[b][kStPy1][e][lane], &F.psi1[pi]);
+              }
+              if (kl[e]) {
+                const long long pi = cpml_at<true>(g, 1, 2, F.p, s, q, i, j, k);
+                F.w2[pi] = pml_weight_v(ez[e], a.inv_dy, up, T(-1), pr, sg[b][kStPy2][e][lane], &F.psi2[pi]);
+              }
+            }
+            if (ez_on) {
+              const Face<T>& F = ezlo ? a.eF[4] : a.eF[5];
+              const int q = ezq[e];
+              const Prof<T> pr = prof(F, q);
+              if (il) {
+                const long long pi = cpml_at<true>(g, 2, 1, F.p, s, q, i, j, k);
+                F.w1[pi] = pml_weight_v(ex[e], a.inv_dz, up, T(-1), pr, sg[b][kStPz1][e][lane], &F.psi1[pi]);
+              }
+              if (jl) {
+                const long long pi = cpml_at<true>(g, 2, 2, F.p, s, q, i, j, k);
+                F.w2[pi] = pml_weight_v(ey[e], a.inv_dz, up, T(1), pr, sg[b][kStPz2][e][lane], &F.psi2[pi]);
+              }
+            }
+          }
+        }
+      } else if (pml) {
+#pragma unroll
+        for (int e = 0; e < 2; ++e)
+          if (kv[e]) e_pml_head(a, s, i, j, kof[e], (i * NY + j) * NZ + kof[e], ex[e], ey[e], ez[e]);
+      }
+    }
+    if (kv[1]) {
+      st2(lEx + o + row, ex);
+      st2(lEy + o + row, ey);
+      st2(lEz + o + row, ez);
+    } else if (kv[0]) {
+      lEx[o + row] = ex[0];
+      lEy[o + row] = ey[0];
+      lEz[o + row] = ez[0];
+    }
+#pragma unroll
+    for (int m = 0; m < 2 * R - 1; ++m)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        qA[m][e] = qA[m + 1][e];
+        qB[m][e] = qB[m + 1][e];
+      }
+  }
+}
+
+// Head of reverse step nt-1 at every cell (receiver cotangents, staged source
+// terms, E-CPML weights); runs once before the reverse loop.
+template <typename T>
+__global__ void __launch_bounds__(32 * K3_WARPS) k3v_adj_head(TiledAdj<T> P, K3Buf<T> f, K3Geom kg) {
+  const AdjArgs<T>& a = P.a;
+  const Grid& g = a.g;
+  const K3Pos wp = k3_pos(kg, g);
+  if (!wp.live) return;
+  const int NX = g.NX, NY = g.NY, NZ = g.NZ, zp = kg.zp, s = wp.s, j = wp.j, kk = wp.kk;
+  const int PS = NY * zp;
+  const long long sbase = (long long)s * NX * PS;
+  const int st = a.ctrl->cur;
+  for (int i = wp.x0; i < wp.x1; ++i) {
+    const long long o = sbase + (long long)i * PS + j * zp;
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      const int k = kk + e;
+      if (k >= NZ) continue;
+      T ex = f.Ex[o + k], ey = f.Ey[o + k], ez = f.Ez[o + k];
+      const int c = (i * NY + j) * NZ + k;
+      tiled_head(P, st, s, c, ex, ey, ez);
+      if (a.has_cpml) e_pml_head(a, s, i, j, k, c, ex, ey, ez);
+      f.Ex[o + k] = ex;
+      f.Ey[o + k] = ey;
+      f.Ez[o + k] = ez;
+    }
+  }
+}
+
+}  // namespace dg

@@ -39,6 +39,7 @@ struct AdjArgs {
   T dx, dy, dz;
   T inv_dx, inv_dy, inv_dz;         // 1/spacing as the reference forms it
   FixedDiv<T> ddt;                  // division by dt (imaging condition)
+  FixedDiv<T> ddy, ddz;             // division by dy, dz (curl scaling c dx / d)
   int dy_eq, dz_eq;
   T *lEx, *lEy, *lEz, *lHx, *lHy, *lHz;
   const T *ce_hist, *ce_curl, *ce_rhs, *ch_curl, *ch_rhs;

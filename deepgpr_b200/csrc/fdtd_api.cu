@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "fdtd_3d.cuh"
+#include "fdtd_3d_adj.cuh"
 
 #define DGB_API extern "C" __attribute__((visibility("default")))
 
@@ -1205,6 +1206,8 @@ void backward_impl(const BackwardCall<T>& bc) {
     a.dy = cm.dy;
     a.dz = cm.dz;
     a.ddt = fixed_div(cm.dt);
+    a.ddy = fixed_div(cm.dy);
+    a.ddz = fixed_div(cm.dz);
     a.inv_dx = T(1) / cm.dx;
     a.inv_dy = T(1) / cm.dy;
     a.inv_dz = T(1) / cm.dz;
@@ -1283,18 +1286,23 @@ void backward_impl(const BackwardCall<T>& bc) {
     TmGeom tg;
     memset(&tg, 0, sizeof(tg));
     if (tm2d) tg = tm_layout(g);
+    K3Geom kg;
+    memset(&kg, 0, sizeof(kg));
     std::vector<char> src_any, rcv_any;
+    const unsigned char *src_rows = nullptr, *rcv_rows = nullptr;
     if (ok && a.want_src) {
       a.srcv = scratch.get<T>((size_t)g.nshot * bc.nsrc * sizeof(T));
       ok = a.srcv != nullptr;
       if (ok) cudaMemsetAsync(a.srcv, 0, (size_t)g.nshot * bc.nsrc * sizeof(T), st);
       if (ok)
         ok = build_pointset(bc.src_loc, g.nshot, bc.nsrc, g, st, scratch, &P.src, &a.src, "source", kErrSourceRange,
-                            tm2d ? &tg.src_rows : nullptr, tm2d ? &src_any : nullptr);
+                            &src_rows, tm2d ? &src_any : nullptr);
     }
     if (ok && bc.rx_comp >= 0 && bc.rx_comp <= 2)
       ok = build_pointset(bc.rx_loc, g.nshot, bc.ndata, g, st, scratch, &P.rcv, &a.rcv, "receiver", kErrReceiverRange,
-                          tm2d ? &tg.rcv_rows : nullptr, tm2d ? &rcv_any : nullptr);
+                          &rcv_rows, tm2d ? &rcv_any : nullptr);
+    tg.src_rows = src_rows;
+    tg.rcv_rows = rcv_rows;
     // rows with a receiver or source of any shot go to the general (frame) kernels
     std::vector<char> pt_rows(tm2d ? g.NX : 0, 0);
     for (int i = 0; i < (int)pt_rows.size(); ++i)
@@ -1344,6 +1352,30 @@ void backward_impl(const BackwardCall<T>& bc) {
         ok = cuda_ok(cudaGetLastError(), "pack");
       }
     }
+    // 3D: lambda and coefficients in the z-pitched working copy
+    K3Buf<T> kb;
+    memset(&kb, 0, sizeof(kb));
+    if (ok && !tm2d) {
+      kg = k3_layout(g);
+      kg.src_rows = src_rows;
+      kg.rcv_rows = rcv_rows;
+      const int* pf = cm.p;
+      kg.cpml_single = g.NX >= pf[0] + pf[1] + 4 && g.NY >= pf[2] + pf[3] + 4 && g.NZ >= pf[4] + pf[5] + 4;
+      ok = k3_alloc_pack(scratch, g, kg, cm, st, kb, bc.lEx, bc.lEy, bc.lEz, bc.lHx, bc.lHy, bc.lHz);
+    }
+    const dim3 kblock(32, K3_WARPS);
+    const int ksmem = k3_adj_smem_bytes<T>();
+    if (ok && !tm2d) {
+      // the double-precision stages exceed the 48 KB default
+      const void* fns[12] = {
+          (const void*)k3v_adj_e<T, 1, false>, (const void*)k3v_adj_e<T, 2, false>, (const void*)k3v_adj_e<T, 4, false>,
+          (const void*)k3v_adj_h<T, 1, false>, (const void*)k3v_adj_h<T, 2, false>, (const void*)k3v_adj_h<T, 4, false>,
+          (const void*)k3v_adj_e<T, 1, true>,  (const void*)k3v_adj_e<T, 2, true>,  (const void*)k3v_adj_e<T, 4, true>,
+          (const void*)k3v_adj_h<T, 1, true>,  (const void*)k3v_adj_h<T, 2, true>,  (const void*)k3v_adj_h<T, 4, true>};
+      for (const void* fn : fns)
+        if (ok) ok = cuda_ok(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, ksmem),
+                             "adjoint shared memory attribute");
+    }
     if (ok && cm.nt > 0) {
       a.ctrl = ctrl;
       k_set<<<1, 1, 0, st>>>(ctrl, cm.nt - 1);
@@ -1365,9 +1397,6 @@ void backward_impl(const BackwardCall<T>& bc) {
       P.xchunk = pick_xchunk(g.NX, tiles, g.nshot, 4 * R);
       dim3 grid((unsigned)tiles, (unsigned)((g.NX + P.xchunk - 1) / P.xchunk), (unsigned)g.nshot);
       const unsigned img_blocks = (unsigned)((a.box.cells() + 255) / 256);
-      const T* lamx = bc.lEx;
-      const T* lamy = bc.lEy;
-      const T* lamz = bc.lEz;
       // head of step nt-1
       {
         TiledAdj<T> b = P;
@@ -1379,9 +1408,7 @@ void backward_impl(const BackwardCall<T>& bc) {
           else if (R == 2) tm_adj_h<T, 2, true><<<gP, wblock, 0, st>>>(b, tl, fP);
           else tm_adj_h<T, 4, true><<<gP, wblock, 0, st>>>(b, tl, fP);
         } else {
-          if (R == 1) k3_adj_h<T, 1, true><<<grid, 256, 0, st>>>(b);
-          else if (R == 2) k3_adj_h<T, 2, true><<<grid, 256, 0, st>>>(b);
-          else k3_adj_h<T, 4, true><<<grid, 256, 0, st>>>(b);
+          k3v_adj_head<T><<<(unsigned)kg.nblocks, kblock, 0, st>>>(b, kb, kg);
         }
         ok = cuda_ok(cudaGetLastError(), "adjoint prologue");
       }
@@ -1392,7 +1419,10 @@ void backward_impl(const BackwardCall<T>& bc) {
           if (tm2d)
             timed(KK_IMAGE, st, [&] { launch_tm_image<T>(kind, a.e_only != 0, a.acc64 != 0, st, b.a, tl.Ez, tg); });
           else
-            timed(KK_IMAGE, st, [&] { k_image<T><<<img_blocks, 256, 0, st>>>(b.a, lamx, lamy, lamz); });
+            timed(KK_IMAGE, st, [&] {
+              k_image<T><<<img_blocks, 256, 0, st>>>(b.a, kb.Ex, kb.Ey, kb.Ez, (long long)g.NX * g.NY * kg.zp,
+                                                     g.NY * kg.zp, kg.zp);
+            });
         }
         if (tm2d) {
           timed(KK_ADJ_E, st, [&] {
@@ -1428,19 +1458,34 @@ void backward_impl(const BackwardCall<T>& bc) {
                 });
           });
         } else {
+          const unsigned nb = (unsigned)kg.nblocks;
+          const bool eq3 = cm.dy == cm.dx && cm.dz == cm.dx;
           timed(KK_ADJ_E, st, [&] {
-            if (R == 1) k3_adj_e<T, 1><<<grid, 256, 0, st>>>(b);
-            else if (R == 2) k3_adj_e<T, 2><<<grid, 256, 0, st>>>(b);
-            else k3_adj_e<T, 4><<<grid, 256, 0, st>>>(b);
+            if (eq3) {
+              if (R == 1) k3v_adj_e<T, 1, true><<<nb, kblock, ksmem, st>>>(b, kb, kg);
+              else if (R == 2) k3v_adj_e<T, 2, true><<<nb, kblock, ksmem, st>>>(b, kb, kg);
+              else k3v_adj_e<T, 4, true><<<nb, kblock, ksmem, st>>>(b, kb, kg);
+            } else {
+              if (R == 1) k3v_adj_e<T, 1, false><<<nb, kblock, ksmem, st>>>(b, kb, kg);
+              else if (R == 2) k3v_adj_e<T, 2, false><<<nb, kblock, ksmem, st>>>(b, kb, kg);
+              else k3v_adj_e<T, 4, false><<<nb, kblock, ksmem, st>>>(b, kb, kg);
+            }
           });
           timed(KK_ADJ_H, st, [&] {
-            if (R == 1) k3_adj_h<T, 1, false><<<grid, 256, 0, st>>>(b);
-            else if (R == 2) k3_adj_h<T, 2, false><<<grid, 256, 0, st>>>(b);
-            else k3_adj_h<T, 4, false><<<grid, 256, 0, st>>>(b);
+            if (eq3) {
+              if (R == 1) k3v_adj_h<T, 1, true><<<nb, kblock, ksmem, st>>>(b, kb, kg);
+              else if (R == 2) k3v_adj_h<T, 2, true><<<nb, kblock, ksmem, st>>>(b, kb, kg);
+              else k3v_adj_h<T, 4, true><<<nb, kblock, ksmem, st>>>(b, kb, kg);
+            } else {
+              if (R == 1) k3v_adj_h<T, 1, false><<<nb, kblock, ksmem, st>>>(b, kb, kg);
+              else if (R == 2) k3v_adj_h<T, 2, false><<<nb, kblock, ksmem, st>>>(b, kb, kg);
+              else k3v_adj_h<T, 4, false><<<nb, kblock, ksmem, st>>>(b, kb, kg);
+            }
           });
         }
       };
       if (ok) ok = run_loop(cm.nt, -1, ctrl, st, issue);
+      if (ok && !tm2d) ok = k3_unpack(g, kg, st, kb, bc.lEx, bc.lEy, bc.lEz, bc.lHx, bc.lHy, bc.lHz);
       if (ok && tm2d) {
         k_unpack2d_pitch<T><<<2048, 256, 0, st>>>(tl.Ez, bc.lEz, (long long)g.nshot * g.NX, g.NY, tg.NYP);
         k_unpack2d_pitch<T><<<2048, 256, 0, st>>>(tl.Hx, bc.lHx, (long long)g.nshot * g.NX, g.NY, tg.NYP);

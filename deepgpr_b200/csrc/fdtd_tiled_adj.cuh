@@ -418,10 +418,12 @@ __global__ void __launch_bounds__(256) k3_adj_h(TiledAdj<T> P) {
 // Imaging condition of one saved step (deepgpr_cpu.c:1659-1745).
 // One thread per history-box cell; shots and components summed inside the
 // thread in the reference's order.  lam_* point at lambda_E before the
-// ce_hist scaling of this step.  3D grids (the 2D TM path uses tm_image).
+// ce_hist scaling of this step, element (s, i, j, k) at
+// s * ls + i * lp + j * lr + k.  3D grids (the 2D TM path uses tm_image).
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(256) k_image(AdjArgs<T> a, const T* lam_x, const T* lam_y, const T* lam_z) {
+__global__ void __launch_bounds__(256) k_image(AdjArgs<T> a, const T* lam_x, const T* lam_y, const T* lam_z,
+                                               long long ls, int lp, int lr) {
   const Grid& g = a.g;
   const int it = a.ctrl->cur - a.k_in_chunk;
   if (it % a.S != 0) return;
@@ -433,8 +435,7 @@ __global__ void __launch_bounds__(256) k_image(AdjArgs<T> a, const T* lam_x, con
   const int rem = int(hidx % ((long long)a.box.ny * a.box.nz));
   const int i = hi + a.box.x0, j = rem / a.box.nz + a.box.y0, k = rem % a.box.nz + a.box.z0;
   const int c = i * g.sx + j * g.NZ + k;
-  const int cl = c;
-  const long long lcells = g.cells;
+  const long long cl = (long long)i * lp + (long long)j * lr + k;
   const T ca = a.ce_hist[c], cbv = a.ce_rhs[c];
   int w = a.S;
   if (it + w > a.nt) w = a.nt - it;
@@ -451,7 +452,7 @@ __global__ void __launch_bounds__(256) k_image(AdjArgs<T> a, const T* lam_x, con
   T loc_e = T(0), loc_s = T(0);
   double loc_e64 = 0.0, loc_s64 = 0.0;
   for (int s = 0; s < g.nshot; ++s) {
-    const long long lf = (long long)s * lcells + cl;
+    const long long lf = (long long)s * ls + cl;
     for (int q = 0; q < ncomp; ++q) {
       const int fc = a.mode == 3 ? q : 2;
       const bool du = fc == 0 ? dex : (fc == 1 ? dey : dez);
