@@ -284,7 +284,7 @@ constexpr int kStageSlots = 7;
 // ---------------------------------------------------------------------------
 // 3D H half step (+ E^n history).  EQ: dx == dy == dz (curl scale 1).
 // ---------------------------------------------------------------------------
-template <typename T, int R, bool EQ>
+template <typename T, int R, bool EQ, bool GEN>
 __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 : 3) k3v_fwd_h(TiledFwd<T> P, K3Buf<T> f, K3Geom kg) {
   constexpr int ZLO = -(R - 1), ZHI = R + 1, NZN = ZHI - ZLO + 1;   // z neighbours of the pair, dfwd
   const FwdArgs<T>& a = P.a;
@@ -330,7 +330,7 @@ __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 
   const int qy1 = a.has_cpml ? q_high(a.hF[3].p, j, NY) : -1;
   const bool in_y = qy0 >= 0 || qy1 >= 0;
   // CPML rows of the row's y face and the lane's z face (faces of one axis apart)
-  const bool cps = a.has_cpml && kg.cpml_single;
+  const bool cps = !GEN && a.has_cpml;   // GEN: faces of an axis may meet (general form)
   const int fz = (qz0[0] >= 0 || qz0[1] >= 0) ? 4 : 5;
   int zq[2];
 #pragma unroll
@@ -547,7 +547,7 @@ __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 
           cpml_one<T>(zr.p2, (long long)i * zr.s2 + zq[e], sg[b][5][e][lane], pr, dEx_dz[e], a.ddz, up[e], false,
                       hy[e]);
       }
-    } else if (in_x || in_y || any_zpml) {
+    } else if (GEN && (in_x || in_y || any_zpml)) {
       // faces of one axis meet: the general per-face form
       T up[2];
       bool zon[2];
@@ -636,7 +636,7 @@ __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 
 // ---------------------------------------------------------------------------
 // 3D E half step (+ sources, R^n history, receivers).
 // ---------------------------------------------------------------------------
-template <typename T, int R, bool EQ>
+template <typename T, int R, bool EQ, bool GEN>
 __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 : 3) k3v_fwd_e(TiledFwd<T> P, K3Buf<T> f, K3Geom kg) {
   constexpr int ZLO = -R, ZHI = R, NZN = ZHI - ZLO + 1;   // z neighbours of the pair, dback
   const FwdArgs<T>& a = P.a;
@@ -690,7 +690,7 @@ __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 
   const long long bplane = (long long)a.box.ny * a.box.nz;
   const long long h0 = (long long)(j - a.box.y0) * a.box.nz + (kk - a.box.z0);
   const long long hb = slot * a.frame + s * a.box.cells();
-  const bool cps = a.has_cpml && kg.cpml_single;
+  const bool cps = !GEN && a.has_cpml;   // GEN: faces of an axis may meet (general form)
   const int fz = (qz0[0] >= 0 || qz0[1] >= 0) ? 4 : 5;
   int zq[2];
 #pragma unroll
@@ -888,7 +888,7 @@ __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 
           cpml_one<T>(zr.p2, (long long)i * zr.s2 + zq[e], sg[b][5][e][lane], pr, dHx_dz[e], a.ddz, cb[e], true,
                       ey[e]);
       }
-    } else if (in_x || in_y || any_zpml) {
+    } else if (GEN && (in_x || in_y || any_zpml)) {
       // faces of one axis meet: the general per-face form
       const bool jl = j < NY - 1, il = i < NX - 1;
       const bool onk[2] = {kl[0], kl[1]}, onj[2] = {kv[0] && jl, kv[1] && jl}, oni[2] = {kv[0] && il, kv[1] && il};

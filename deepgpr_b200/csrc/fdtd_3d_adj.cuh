@@ -127,6 +127,63 @@ __device__ __forceinline__ T curl_z(const AdjArgs<T>& a, T c) {
   return (EQ || a.dz_eq) ? c : div_fixed(c * a.dx, a.ddz);
 }
 
+// General-form CPML pieces, out of line: a call is never predicated, so
+// these lookups cost nothing on the planes and rows that do not take them
+// (the kernels' parameter block is __grid_constant__, so references into it
+// are passed without a copy).
+// CPML weight of a source cell from the faces lo, hi of an axis (0 + lo + hi,
+// add_pml of fdtd_adjoint.cuh).
+template <typename T, bool EFACE>
+__device__ __noinline__ T pml_w_gen(const Face<T>& lo, const Face<T>& hi, const Grid& g, int axis, int slot, int s,
+                                    int i, int j, int k) {
+  T w = T(0);
+  add_pml<T, EFACE>(w, lo, hi, g, axis, slot, s, i, j, k);
+  return w;
+}
+// H-CPML adjoint weights of one cell, every face in turn (deepgpr_cpu.c:1331-1396)
+template <typename T>
+__device__ __noinline__ void h_weights_gen(const AdjArgs<T>& a, int s, int i, int j, int k, T up, T hx, T hy,
+                                           T hz) {
+  const Grid& g = a.g;
+  int qh[6];
+  face_q<false>(a.hF[0].p, a.hF[1].p, i, g.NX, qh[0], qh[1]);
+  face_q<false>(a.hF[2].p, a.hF[3].p, j, g.NY, qh[2], qh[3]);
+  face_q<false>(a.hF[4].p, a.hF[5].p, k, g.NZ, qh[4], qh[5]);
+  const bool il = i < g.NX - 1, jl = j < g.NY - 1, kl = k < g.NZ - 1;
+#pragma unroll
+  for (int fc = 0; fc < 6; ++fc) {
+    const int q = qh[fc];
+    if (q < 0) continue;
+    const Face<T>& F = a.hF[fc];
+    const Prof<T> pr = prof(F, q);
+    const int axis = fc >> 1;
+    const bool on1 = axis == 2 ? jl : kl;
+    const bool on2 = axis == 0 ? jl : il;
+    const T l1 = axis == 0 ? hy : hx;
+    const T l2 = axis == 2 ? hy : hz;
+    const T ih = axis == 0 ? a.inv_dx : (axis == 1 ? a.inv_dy : a.inv_dz);
+    const T s1 = axis == 1 ? T(-1) : T(1);
+    const T s2 = axis == 1 ? T(1) : T(-1);
+    if (on1) {
+      const long long pi = cpml_at<false>(g, axis, 1, F.p, s, q, i, j, k);
+      F.w1[pi] = pml_weight(l1, ih, up, s1, pr, &F.psi1[pi]);
+    }
+    if (on2) {
+      const long long pi = cpml_at<false>(g, axis, 2, F.p, s, q, i, j, k);
+      F.w2[pi] = pml_weight(l2, ih, up, s2, pr, &F.psi2[pi]);
+    }
+  }
+}
+// head of a reverse step at one cell: receivers, sources, E-CPML weights
+template <typename T>
+__device__ __noinline__ void head_gen(const TiledAdj<T>& P, int st, int s, int i, int j, int k, bool pts, bool epml,
+                                      T& ex, T& ey, T& ez) {
+  const Grid& g = P.a.g;
+  const int c = (i * g.NY + j) * g.NZ + k;
+  if (pts) tiled_head(P, st, s, c, ex, ey, ez);
+  if (epml) e_pml_head(P.a, s, i, j, k, c, ex, ey, ez);
+}
+
 // stage slots of the adjoint kernels
 constexpr int kAdjSlots = 13;
 enum : int {
@@ -151,9 +208,9 @@ constexpr int k3_adj_smem_bytes() {
 //   C_Y = y faces w2 + (-c_y) lambda_ez, C_Z = z faces w2 + c_z lambda_ey  -> lambda_hx
 // then the H-CPML weights of step it at the cell (deepgpr_cpu.c:1331-1396).
 // ---------------------------------------------------------------------------
-template <typename T, int R, bool EQ>
+template <typename T, int R, bool EQ, bool GEN>
 __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 : 3)
-    k3v_adj_e(TiledAdj<T> P, K3Buf<T> f, K3Geom kg) {
+    k3v_adj_e(const __grid_constant__ TiledAdj<T> P, K3Buf<T> f, K3Geom kg) {
   constexpr int ZLO = -(R - 1), ZHI = R + 1, NZN = ZHI - ZLO + 1;   // z sources of the pair, gather_back
   const AdjArgs<T>& a = P.a;
   const Grid& g = a.g;
@@ -182,7 +239,8 @@ __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 
   const bool hok = lane < 2 * R && hk >= 0 && hk < NZ;
   const int row = j * zp + kk;
   const int hrow = j * zp + (hok ? hk : 0);
-  const bool pml = a.has_cpml != 0, cps = pml && kg.cpml_single;
+  // GEN: faces of an axis may meet (general form); else one face per axis (staged)
+  const bool pml = a.has_cpml != 0, cps = !GEN && pml;
   // parts of the interior predicates (upd_e*): mid = 0 < c < n-1, lo = c < n-1
   const bool dxo = NY - 1 != 1 || NZ - 1 != 1, dyo = NX - 1 != 1 || NZ - 1 != 1, dzo = NX - 1 != 1 || NY - 1 != 1;
   const bool jm = j > 0 && j < NY - 1, jl = j < NY - 1;
@@ -324,9 +382,9 @@ __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 
         if (cps) {
           if (jl && kv[e]) wa += sg[b][kStXw1][e][lane];
           if (kl[e]) wb += sg[b][kStXw2][e][lane];
-        } else {
-          if (jl && kv[e]) add_pml<T, true>(wa, a.eF[0], a.eF[1], g, 0, 1, s, x, j, kof[e]);
-          if (kl[e]) add_pml<T, true>(wb, a.eF[0], a.eF[1], g, 0, 2, s, x, j, kof[e]);
+        } else if (GEN) {
+          if (jl && kv[e]) wa = pml_w_gen<T, true>(a.eF[0], a.eF[1], g, 0, 1, s, x, j, kof[e]);
+          if (kl[e]) wb = pml_w_gen<T, true>(a.eF[0], a.eF[1], g, 0, 2, s, x, j, kof[e]);
         }
       }
       if (dyo && xm && jl && km[e]) wa += (-c[e]) * ly[e];
@@ -353,8 +411,8 @@ __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 
     for (int e = 0; e < 2; ++e) {
       T wa = T(0), wb = T(0);
       if (pml && pl >= 0 && pl < NX) {
-        if (jl && kv[e]) add_pml<T, true>(wa, a.eF[0], a.eF[1], g, 0, 1, s, pl, j, kof[e]);
-        if (kl[e]) add_pml<T, true>(wb, a.eF[0], a.eF[1], g, 0, 2, s, pl, j, kof[e]);
+        if (jl && kv[e]) wa = pml_w_gen<T, true>(a.eF[0], a.eF[1], g, 0, 1, s, pl, j, kof[e]);
+        if (kl[e]) wb = pml_w_gen<T, true>(a.eF[0], a.eF[1], g, 0, 2, s, pl, j, kof[e]);
       }
       if (dyo && xm && jl && km[e]) wa += (-c[e]) * ly[e];
       if (dzo && xm && jm && kl[e]) wb += c[e] * lz[e];
@@ -426,9 +484,9 @@ __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 
       if (cps) {
         if (ezq[e] >= 0 && il) w1 += sg[b][kStZw1][e][lane];
         if (ezq[e] >= 0 && jl) w2 += sg[b][kStZw2][e][lane];
-      } else if (pml && kv[e]) {
-        if (il) add_pml<T, true>(w1, a.eF[4], a.eF[5], g, 2, 1, s, i, j, kof[e]);
-        if (jl) add_pml<T, true>(w2, a.eF[4], a.eF[5], g, 2, 2, s, i, j, kof[e]);
+      } else if (GEN && pml && kv[e]) {
+        if (il) w1 = pml_w_gen<T, true>(a.eF[4], a.eF[5], g, 2, 1, s, i, j, kof[e]);
+        if (jl) w2 = pml_w_gen<T, true>(a.eF[4], a.eF[5], g, 2, 2, s, i, j, kof[e]);
       }
       const T cze = curl_z<EQ>(a, c[e]);
       if (dxo && il && jm && km[e]) w1 += (-cze) * ex[e];
@@ -440,9 +498,9 @@ __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 
       if (cps) {
         if (ehq >= 0 && il) hbz += sg[b][kStHw1][0][lane];
         if (ehq >= 0 && jl) hcz += sg[b][kStHw2][0][lane];
-      } else if (pml) {
-        if (il) add_pml<T, true>(hbz, a.eF[4], a.eF[5], g, 2, 1, s, i, j, hk);
-        if (jl) add_pml<T, true>(hcz, a.eF[4], a.eF[5], g, 2, 2, s, i, j, hk);
+      } else if (GEN && pml) {
+        if (il) hbz = pml_w_gen<T, true>(a.eF[4], a.eF[5], g, 2, 1, s, i, j, hk);
+        if (jl) hcz = pml_w_gen<T, true>(a.eF[4], a.eF[5], g, 2, 2, s, i, j, hk);
       }
       const T czh = curl_z<EQ>(a, hc);
       if (dxo && il && jm && hkm) hbz += (-czh) * hex;
@@ -477,8 +535,8 @@ __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 
       for (int e = 0; e < 2; ++e) {
         T w1 = T(0), w2 = T(0);
         if ((ymask >> m) & 1u) {
-          if (il && kv[e]) add_pml<T, true>(w1, a.eF[2], a.eF[3], g, 1, 1, s, i, y, kof[e]);
-          if (kl[e]) add_pml<T, true>(w2, a.eF[2], a.eF[3], g, 1, 2, s, i, y, kof[e]);
+          if (il && kv[e]) w1 = pml_w_gen<T, true>(a.eF[2], a.eF[3], g, 1, 1, s, i, y, kof[e]);
+          if (kl[e]) w2 = pml_w_gen<T, true>(a.eF[2], a.eF[3], g, 1, 2, s, i, y, kof[e]);
         }
         const T cye = curl_y<EQ>(a, cv[e]);
         if (dxo && il && ym && km[e]) w1 += cye * lx[e];
@@ -563,42 +621,11 @@ __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 
           }
         }
       }
-    } else if (pml) {
+    } else if (GEN && pml) {
       // faces of one axis meet: every face in turn, direct loads
 #pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        if (!kv[e]) continue;
-        const int k = kof[e];
-        int qh[6];
-        face_q<false>(a.hF[0].p, a.hF[1].p, i, NX, qh[0], qh[1]);
-        face_q<false>(a.hF[2].p, a.hF[3].p, j, NY, qh[2], qh[3]);
-        face_q<false>(a.hF[4].p, a.hF[5].p, k, NZ, qh[4], qh[5]);
-        if (qh[0] < 0 && qh[1] < 0 && qh[2] < 0 && qh[3] < 0 && qh[4] < 0 && qh[5] < 0) continue;
-        const T up = f.ch_rhs[o + row + e];
-#pragma unroll
-        for (int fc = 0; fc < 6; ++fc) {
-          const int q = qh[fc];
-          if (q < 0) continue;
-          const Face<T>& F = a.hF[fc];
-          const Prof<T> pr = prof(F, q);
-          const int axis = fc >> 1;
-          const bool on1 = axis == 2 ? jl : kl[e];
-          const bool on2 = axis == 0 ? jl : il;
-          const T l1 = axis == 0 ? hy[e] : hx[e];
-          const T l2 = axis == 2 ? hy[e] : hz[e];
-          const T ih = axis == 0 ? a.inv_dx : (axis == 1 ? a.inv_dy : a.inv_dz);
-          const T s1 = axis == 1 ? T(-1) : T(1);
-          const T s2 = axis == 1 ? T(1) : T(-1);
-          if (on1) {
-            const long long pi = cpml_at<false>(g, axis, 1, F.p, s, q, i, j, k);
-            F.w1[pi] = pml_weight(l1, ih, up, s1, pr, &F.psi1[pi]);
-          }
-          if (on2) {
-            const long long pi = cpml_at<false>(g, axis, 2, F.p, s, q, i, j, k);
-            F.w2[pi] = pml_weight(l2, ih, up, s2, pr, &F.psi2[pi]);
-          }
-        }
-      }
+      for (int e = 0; e < 2; ++e)
+        if (kv[e]) h_weights_gen(a, s, i, j, kof[e], f.ch_rhs[o + row + e], hx[e], hy[e], hz[e]);
     }
 #pragma unroll
     for (int m = 0; m < 2 * R - 1; ++m)
@@ -617,9 +644,9 @@ __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 
 //   C_Y = y faces w2 + c_y lambda_hz,    C_Z = z faces w2 + (-c_z) lambda_hy -> lambda_ex
 // then the head of step it-1 at the cell.
 // ---------------------------------------------------------------------------
-template <typename T, int R, bool EQ>
+template <typename T, int R, bool EQ, bool GEN>
 __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 : 3)
-    k3v_adj_h(TiledAdj<T> P, K3Buf<T> f, K3Geom kg) {
+    k3v_adj_h(const __grid_constant__ TiledAdj<T> P, K3Buf<T> f, K3Geom kg) {
   constexpr int ZLO = -R, ZHI = R, NZN = ZHI - ZLO + 1;   // z sources of the pair, gather_fwd
   const AdjArgs<T>& a = P.a;
   const Grid& g = a.g;
@@ -641,7 +668,8 @@ __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 
   const bool hok = lane < 2 * R && hk >= 0 && hk < NZ;
   const int row = j * zp + kk;
   const int hrow = j * zp + (hok ? hk : 0);
-  const bool pml = a.has_cpml != 0, cps = pml && kg.cpml_single;
+  // GEN: faces of an axis may meet (general form); else one face per axis (staged)
+  const bool pml = a.has_cpml != 0, cps = !GEN && pml;
   // parts of upd_h*: hx: NX-1 != 1, mid(i), lo(j), lo(k); hy: NY-1 != 1, lo(i),
   // mid(j), lo(k); hz: NZ-1 != 1, lo(i), lo(j), mid(k); and of upd_e* for ce_hist
   const bool hxo = NX - 1 != 1, hyo = NY - 1 != 1, hzo = NZ - 1 != 1;
@@ -780,9 +808,9 @@ __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 
         if (cps) {
           if (kl[e]) wa += sg[b][kStXw1][e][lane];
           if (jl && kv[e]) wb += sg[b][kStXw2][e][lane];
-        } else {
-          if (kl[e]) add_pml<T, false>(wa, a.hF[0], a.hF[1], g, 0, 1, s, x, j, kof[e]);
-          if (jl && kv[e]) add_pml<T, false>(wb, a.hF[0], a.hF[1], g, 0, 2, s, x, j, kof[e]);
+        } else if (GEN) {
+          if (kl[e]) wa = pml_w_gen<T, false>(a.hF[0], a.hF[1], g, 0, 1, s, x, j, kof[e]);
+          if (jl && kv[e]) wb = pml_w_gen<T, false>(a.hF[0], a.hF[1], g, 0, 2, s, x, j, kof[e]);
         }
       }
       if (hyo && xl && jm && kl[e]) wa += c[e] * ly[e];
@@ -808,8 +836,8 @@ __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 
     for (int e = 0; e < 2; ++e) {
       T wa = T(0), wb = T(0);
       if (pml && pl >= 0 && pl < NX) {
-        if (kl[e]) add_pml<T, false>(wa, a.hF[0], a.hF[1], g, 0, 1, s, pl, j, kof[e]);
-        if (jl && kv[e]) add_pml<T, false>(wb, a.hF[0], a.hF[1], g, 0, 2, s, pl, j, kof[e]);
+        if (kl[e]) wa = pml_w_gen<T, false>(a.hF[0], a.hF[1], g, 0, 1, s, pl, j, kof[e]);
+        if (jl && kv[e]) wb = pml_w_gen<T, false>(a.hF[0], a.hF[1], g, 0, 2, s, pl, j, kof[e]);
       }
       if (hyo && xl && jm && kl[e]) wa += c[e] * ly[e];
       if (hzo && xl && jl && km[e]) wb += (-c[e]) * lz[e];
@@ -881,9 +909,9 @@ __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 
       if (cps) {
         if (hzq[e] >= 0 && jl) w1 += sg[b][kStZw1][e][lane];
         if (hzq[e] >= 0 && il) w2 += sg[b][kStZw2][e][lane];
-      } else if (pml && kv[e]) {
-        if (jl) add_pml<T, false>(w1, a.hF[4], a.hF[5], g, 2, 1, s, i, j, kof[e]);
-        if (il) add_pml<T, false>(w2, a.hF[4], a.hF[5], g, 2, 2, s, i, j, kof[e]);
+      } else if (GEN && pml && kv[e]) {
+        if (jl) w1 = pml_w_gen<T, false>(a.hF[4], a.hF[5], g, 2, 1, s, i, j, kof[e]);
+        if (il) w2 = pml_w_gen<T, false>(a.hF[4], a.hF[5], g, 2, 2, s, i, j, kof[e]);
       }
       const T cze = curl_z<EQ>(a, c[e]);
       if (hxo && im && jl && kl[e]) w1 += cze * hx[e];
@@ -895,9 +923,9 @@ __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 
       if (cps) {
         if (hhq >= 0 && jl) hbz += sg[b][kStHw1][0][lane];
         if (hhq >= 0 && il) hcz += sg[b][kStHw2][0][lane];
-      } else if (pml) {
-        if (jl) add_pml<T, false>(hbz, a.hF[4], a.hF[5], g, 2, 1, s, i, j, hk);
-        if (il) add_pml<T, false>(hcz, a.hF[4], a.hF[5], g, 2, 2, s, i, j, hk);
+      } else if (GEN && pml) {
+        if (jl) hbz = pml_w_gen<T, false>(a.hF[4], a.hF[5], g, 2, 1, s, i, j, hk);
+        if (il) hcz = pml_w_gen<T, false>(a.hF[4], a.hF[5], g, 2, 2, s, i, j, hk);
       }
       const T czh = curl_z<EQ>(a, hc);
       if (hxo && im && jl && hkl) hbz += czh * hhx;
@@ -931,8 +959,8 @@ __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 
       for (int e = 0; e < 2; ++e) {
         T w1 = T(0), w2 = T(0);
         if ((ymask >> m) & 1u) {
-          if (kl[e]) add_pml<T, false>(w1, a.hF[2], a.hF[3], g, 1, 1, s, i, y, kof[e]);
-          if (il && kv[e]) add_pml<T, false>(w2, a.hF[2], a.hF[3], g, 1, 2, s, i, y, kof[e]);
+          if (kl[e]) w1 = pml_w_gen<T, false>(a.hF[2], a.hF[3], g, 1, 1, s, i, y, kof[e]);
+          if (il && kv[e]) w2 = pml_w_gen<T, false>(a.hF[2], a.hF[3], g, 1, 2, s, i, y, kof[e]);
         }
         const T cye = curl_y<EQ>(a, cv[e]);
         if (hxo && im && yl && kl[e]) w1 += (-cye) * lx[e];
@@ -962,7 +990,7 @@ __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 
       if (pts) {
 #pragma unroll
         for (int e = 0; e < 2; ++e)
-          if (kv[e]) tiled_head(P, head, s, (i * NY + j) * NZ + kof[e], ex[e], ey[e], ez[e]);
+          if (kv[e]) head_gen(P, head, s, i, j, kof[e], true, false, ex[e], ey[e], ez[e]);
       }
       // E-CPML adjoint weights of step it-1
       if (cps) {
@@ -1019,10 +1047,10 @@ __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 
             }
           }
         }
-      } else if (pml) {
+      } else if (GEN && pml) {
 #pragma unroll
         for (int e = 0; e < 2; ++e)
-          if (kv[e]) e_pml_head(a, s, i, j, kof[e], (i * NY + j) * NZ + kof[e], ex[e], ey[e], ez[e]);
+          if (kv[e]) head_gen(P, head, s, i, j, kof[e], false, true, ex[e], ey[e], ez[e]);
       }
     }
     if (kv[1]) {
@@ -1070,6 +1098,141 @@ __global__ void __launch_bounds__(32 * K3_WARPS) k3v_adj_head(TiledAdj<T> P, K3B
       f.Ey[o + k] = ey;
       f.Ez[o + k] = ez;
     }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Imaging condition of one saved step on the 3D working copy (deepgpr_cpu.c:
+// 1659-1745): one thread per history-box cell sums shot by shot, component
+// by component (the reference's order), the terms of lambda_E before this
+// step's ce_hist scaling with E^n and E^{n+1} (E-only) or R^n.  KIND, EONLY,
+// ACC64 and NC (components: 1 for Ez, 3 for mode 3) are fixed at compile
+// time; the shots are read in batches of U, the next batch's loads issued
+// before the current batch is summed.  lambda element (s, i, j, k) sits at
+// s * ls + i * lp + j * lr + k.
+// ---------------------------------------------------------------------------
+constexpr int kImage3Threads = 128;
+
+template <typename T, int KIND, bool EONLY, bool ACC64, int NC>
+__global__ void __launch_bounds__(kImage3Threads) k3_image(AdjArgs<T> a, const T* __restrict__ lx,
+                                                           const T* __restrict__ ly, const T* __restrict__ lz,
+                                                           long long ls, int lp, int lr) {
+  constexpr int U = NC == 1 ? 4 : 2;
+  const Grid& g = a.g;
+  const int it = a.ctrl->cur - a.k_in_chunk;
+  if (it % a.S != 0) return;
+  const int slot = it / a.S;
+  const long long bc = a.box.cells();
+  const long long hidx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (hidx >= bc) return;
+  const unsigned bplane = (unsigned)a.box.ny * (unsigned)a.box.nz;
+  const unsigned hu = (unsigned)hidx;   // box cells < 2^31 (host check)
+  const unsigned bi = hu / bplane, rem = hu - bi * bplane;
+  const unsigned bj = rem / (unsigned)a.box.nz, bk = rem - bj * (unsigned)a.box.nz;
+  const int i = int(bi) + a.box.x0, j = int(bj) + a.box.y0, k = int(bk) + a.box.z0;
+  const int c = i * g.sx + j * g.NZ + k;
+  const T ca = a.ce_hist[c], cbv = a.ce_rhs[c];
+  int w = a.S;
+  if (it + w > a.nt) w = a.nt - it;
+  const T wgt = T(w);
+  const bool pec_ok = a.sigma[c] <= Phys<T>::pec();
+  const T dca_e = div_fixed(Phys<T>::eps0() * (T(1) - ca) * cbv, a.ddt);
+  const T dcb_e = div_fixed(-Phys<T>::eps0() * cbv * cbv, a.ddt);
+  const FixedDiv<T> dcb = fixed_div_dev(cbv);   // shared by the shots
+  const T dca_s = T(-0.5) * (T(1) + ca) * cbv;
+  const T dcb_s = T(-0.5) * cbv * cbv;
+  bool du[NC];
+  const T* lam[NC];
+  if (NC == 3) {
+    du[0] = upd_ex(g, i, j, k);
+    du[1 % NC] = upd_ey(g, i, j, k);
+    du[2 % NC] = upd_ez(g, i, j, k);
+    lam[0] = lx;
+    lam[1 % NC] = ly;
+    lam[2 % NC] = lz;
+  } else {
+    du[0] = upd_ez(g, i, j, k);
+    lam[0] = lz;
+  }
+  const int nshot = g.nshot;
+  const bool last = slot + 1 >= a.nt_saved;   // E-only: E^(n+1) of the last frame is in R_saved
+  const long long lc = (long long)i * lp + (long long)j * lr + k;
+  const void* nbase = (EONLY && !last) ? a.E_saved : a.R_saved;
+  const long long ie0 = (long long)slot * a.frame + hidx;
+  const long long in0 = EONLY ? (last ? hidx : ie0 + a.frame) : ie0;
+  const long long nstride = (EONLY && last) ? a.frame : a.comp_stride;   // next value of component q
+  const long long tile = fp8_tile3(g, i, j, k);
+  T acc_e = T(0), acc_s = T(0);
+  double acc_e64 = 0.0, acc_s64 = 0.0;
+  auto term = [&](int q, T lv, T eo, T sec) {
+    T rhs = sec;
+    if (EONLY) rhs = cbv != T(0) ? div_fixed(sec - (du[q] ? ca : T(1)) * eo, dcb) : T(0);
+    const T lamx = (eo == T(0) && rhs == T(0)) ? T(0) : lv;
+    const T gca = du[q] ? lamx * eo * wgt : T(0);
+    const T gcb = lamx * rhs * wgt;
+    const T te = gca * dca_e + gcb * dcb_e;
+    const T ts = gca * dca_s + gcb * dcb_s;
+    if (ACC64) {
+      acc_e64 += double(te);
+      acc_s64 += double(ts);
+    } else {
+      acc_e += te;
+      acc_s += ts;
+    }
+  };
+  auto load1 = [&](int sh, int q, T& l, T& e, T& n) {
+    float esc = 1.0f, rsc = 1.0f;
+    if (KIND == kFP8) {
+      const long long si = (((long long)q * a.nt_saved + slot) * nshot + sh) * a.ntiles + tile;
+      esc = a.e_scales[si];
+      if (!EONLY) rsc = a.r_scales[si];
+    }
+    l = lam[q][sh * ls + lc];
+    e = hist_load<T>(a.E_saved, q * a.comp_stride + ie0 + sh * bc, KIND, esc);
+    n = hist_load<T>(nbase, q * nstride + in0 + sh * bc, KIND, rsc);
+  };
+  T la[U][NC], ea[U][NC], na[U][NC], lb[U][NC], eb[U][NC], nb[U][NC];
+  const int nfull = nshot / U * U;
+  auto load_batch = [&](int s0, T (&l)[U][NC], T (&e)[U][NC], T (&n)[U][NC]) {
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+#pragma unroll
+      for (int q = 0; q < NC; ++q) load1(s0 + u, q, l[u][q], e[u][q], n[u][q]);
+  };
+  auto sum_batch = [&](const T (&l)[U][NC], const T (&e)[U][NC], const T (&n)[U][NC]) {
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+#pragma unroll
+      for (int q = 0; q < NC; ++q) term(q, l[u][q], e[u][q], n[u][q]);
+  };
+  if (nfull > 0) load_batch(0, la, ea, na);
+  for (int s0 = 0; s0 < nfull; s0 += 2 * U) {
+    if (s0 + U < nfull) load_batch(s0 + U, lb, eb, nb);
+    sum_batch(la, ea, na);
+    if (s0 + U >= nfull) break;
+    if (s0 + 2 * U < nfull) load_batch(s0 + 2 * U, la, ea, na);
+    sum_batch(lb, eb, nb);
+  }
+  for (int sh = nfull; sh < nshot; ++sh) {
+#pragma unroll
+    for (int q = 0; q < NC; ++q) {
+      T l, e, n;
+      load1(sh, q, l, e, n);
+      term(q, l, e, n);
+    }
+  }
+  if (!pec_ok) {
+    acc_e = acc_s = T(0);
+    acc_e64 = acc_s64 = 0.0;
+  }
+  const long long gi = ((long long)i * (g.NY - 1) + j) * (g.NZ - 1) + k;
+  if (a.want_eps) {
+    if (ACC64) a.g_eps64[gi] += acc_e64;
+    else a.g_eps[gi] += acc_e;
+  }
+  if (a.want_sig) {
+    if (ACC64) a.g_sig64[gi] += acc_s64;
+    else a.g_sig[gi] += acc_s;
   }
 }
 

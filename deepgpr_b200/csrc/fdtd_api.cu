@@ -527,6 +527,39 @@ void launch_tm_image(int kind, bool e_only, bool acc64, cudaStream_t st, const A
   }
 }
 
+template <typename T, int KIND, int NC>
+void launch_k3_image_k(bool e_only, bool acc64, cudaStream_t st, const AdjArgs<T>& a, const K3Buf<T>& kb,
+                       long long ls, int lp, int lr) {
+  const unsigned blocks = (unsigned)((a.box.cells() + kImage3Threads - 1) / kImage3Threads);
+  constexpr int B = kImage3Threads;
+  if (e_only) {
+    if (acc64) k3_image<T, KIND, true, true, NC><<<blocks, B, 0, st>>>(a, kb.Ex, kb.Ey, kb.Ez, ls, lp, lr);
+    else k3_image<T, KIND, true, false, NC><<<blocks, B, 0, st>>>(a, kb.Ex, kb.Ey, kb.Ez, ls, lp, lr);
+  } else {
+    if (acc64) k3_image<T, KIND, false, true, NC><<<blocks, B, 0, st>>>(a, kb.Ex, kb.Ey, kb.Ez, ls, lp, lr);
+    else k3_image<T, KIND, false, false, NC><<<blocks, B, 0, st>>>(a, kb.Ex, kb.Ey, kb.Ez, ls, lp, lr);
+  }
+}
+
+// Imaging condition of a 3D solve on the pitched lambda_E of kb.
+template <typename T>
+void launch_k3_image(int kind, bool e_only, bool acc64, int mode, cudaStream_t st, const AdjArgs<T>& a,
+                     const K3Buf<T>& kb, long long ls, int lp, int lr) {
+  auto by_nc = [&](auto K) {
+    constexpr int KD = decltype(K)::value;
+    if (mode == 3) launch_k3_image_k<T, KD, 3>(e_only, acc64, st, a, kb, ls, lp, lr);
+    else launch_k3_image_k<T, KD, 1>(e_only, acc64, st, a, kb, ls, lp, lr);
+  };
+  if constexpr (sizeof(T) == 8) {
+    by_nc(std::integral_constant<int, kF64>());
+  } else {
+    if (kind == kF16) by_nc(std::integral_constant<int, kF16>());
+    else if (kind == kBF16) by_nc(std::integral_constant<int, kBF16>());
+    else if (kind == kFP8) by_nc(std::integral_constant<int, kFP8>());
+    else by_nc(std::integral_constant<int, kF32>());
+  }
+}
+
 // One 2D TM half step: the frame kernel on the side stream, forked from and
 // joined back to st, beside the interior kernel on st.  Returns the number
 // of kernels launched.
@@ -551,6 +584,30 @@ dim3 tm_grid(const TmGeom& tg) { return dim3((unsigned)std::max<long long>(1, (t
 
 // 3D working copy: z pitch, strips, y tiles and x chunks.  The chunking keeps
 // the last wave of CTAs nearly full (occupancy of the forward H kernel).
+// Calls f(R, EQ, GEN) with compile-time constants (std::integral_constant)
+// for the runtime stencil radius, "dy == dz == dx" and "CPML faces of an axis
+// may meet".  Double precision (the FP64 runs) is built for the general form
+// only: per-axis curl scales and per-face CPML.
+template <typename T, typename F>
+void k3_variant(int R, bool eq, bool gen, F&& f) {
+  auto by_r = [&](auto E, auto G) {
+    if (R == 1) f(std::integral_constant<int, 1>(), E, G);
+    else if (R == 2) f(std::integral_constant<int, 2>(), E, G);
+    else f(std::integral_constant<int, 4>(), E, G);
+  };
+  if constexpr (sizeof(T) == 8) {
+    by_r(std::false_type(), std::true_type());
+  } else {
+    if (gen) {
+      if (eq) by_r(std::true_type(), std::true_type());
+      else by_r(std::false_type(), std::true_type());
+    } else {
+      if (eq) by_r(std::true_type(), std::false_type());
+      else by_r(std::false_type(), std::false_type());
+    }
+  }
+}
+
 K3Geom k3_layout(const Grid& g) {
   K3Geom kg;
   memset(&kg, 0, sizeof(kg));
@@ -558,7 +615,7 @@ K3Geom k3_layout(const Grid& g) {
   kg.nzs = (g.NZ + K3W - 1) / K3W;
   kg.nyt = (g.NY + K3_WARPS - 1) / K3_WARPS;
   int blocks = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k3v_fwd_h<float, 2, true>, 32 * K3_WARPS, 0) !=
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k3v_fwd_h<float, 2, true, false>, 32 * K3_WARPS, 0) !=
           cudaSuccess ||
       blocks < 1) {
     cudaGetLastError();
@@ -1049,27 +1106,16 @@ void forward_impl(const ForwardCall<T>& fc) {
           });
         } else {
           const dim3 g3((unsigned)kg.nblocks), b3(32, K3_WARPS);
+          const bool gen = a.has_cpml && !kg.cpml_single;
           timed(KK_FWD_H, st, [&] {
-            if (eq3) {
-              if (R == 1) k3v_fwd_h<T, 1, true><<<g3, b3, 0, st>>>(b, kf, kg);
-              else if (R == 2) k3v_fwd_h<T, 2, true><<<g3, b3, 0, st>>>(b, kf, kg);
-              else k3v_fwd_h<T, 4, true><<<g3, b3, 0, st>>>(b, kf, kg);
-            } else {
-              if (R == 1) k3v_fwd_h<T, 1, false><<<g3, b3, 0, st>>>(b, kf, kg);
-              else if (R == 2) k3v_fwd_h<T, 2, false><<<g3, b3, 0, st>>>(b, kf, kg);
-              else k3v_fwd_h<T, 4, false><<<g3, b3, 0, st>>>(b, kf, kg);
-            }
+            k3_variant<T>(R, eq3, gen, [&](auto RR, auto E, auto G) {
+              k3v_fwd_h<T, decltype(RR)::value, decltype(E)::value, decltype(G)::value><<<g3, b3, 0, st>>>(b, kf, kg);
+            });
           });
           timed(KK_FWD_E, st, [&] {
-            if (eq3) {
-              if (R == 1) k3v_fwd_e<T, 1, true><<<g3, b3, 0, st>>>(b, kf, kg);
-              else if (R == 2) k3v_fwd_e<T, 2, true><<<g3, b3, 0, st>>>(b, kf, kg);
-              else k3v_fwd_e<T, 4, true><<<g3, b3, 0, st>>>(b, kf, kg);
-            } else {
-              if (R == 1) k3v_fwd_e<T, 1, false><<<g3, b3, 0, st>>>(b, kf, kg);
-              else if (R == 2) k3v_fwd_e<T, 2, false><<<g3, b3, 0, st>>>(b, kf, kg);
-              else k3v_fwd_e<T, 4, false><<<g3, b3, 0, st>>>(b, kf, kg);
-            }
+            k3_variant<T>(R, eq3, gen, [&](auto RR, auto E, auto G) {
+              k3v_fwd_e<T, decltype(RR)::value, decltype(E)::value, decltype(G)::value><<<g3, b3, 0, st>>>(b, kf, kg);
+            });
           });
         }
       };
@@ -1365,16 +1411,18 @@ void backward_impl(const BackwardCall<T>& bc) {
     }
     const dim3 kblock(32, K3_WARPS);
     const int ksmem = k3_adj_smem_bytes<T>();
+    const bool eq3 = cm.dy == cm.dx && cm.dz == cm.dx;
+    const bool gen3 = has_cpml && !kg.cpml_single;
     if (ok && !tm2d) {
       // the double-precision stages exceed the 48 KB default
-      const void* fns[12] = {
-          (const void*)k3v_adj_e<T, 1, false>, (const void*)k3v_adj_e<T, 2, false>, (const void*)k3v_adj_e<T, 4, false>,
-          (const void*)k3v_adj_h<T, 1, false>, (const void*)k3v_adj_h<T, 2, false>, (const void*)k3v_adj_h<T, 4, false>,
-          (const void*)k3v_adj_e<T, 1, true>,  (const void*)k3v_adj_e<T, 2, true>,  (const void*)k3v_adj_e<T, 4, true>,
-          (const void*)k3v_adj_h<T, 1, true>,  (const void*)k3v_adj_h<T, 2, true>,  (const void*)k3v_adj_h<T, 4, true>};
-      for (const void* fn : fns)
-        if (ok) ok = cuda_ok(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, ksmem),
-                             "adjoint shared memory attribute");
+      k3_variant<T>(R, eq3, gen3, [&](auto RR, auto E, auto G) {
+        constexpr int r = decltype(RR)::value;
+        constexpr bool e = decltype(E)::value, gn = decltype(G)::value;
+        const void* fns[2] = {(const void*)k3v_adj_e<T, r, e, gn>, (const void*)k3v_adj_h<T, r, e, gn>};
+        for (const void* fn : fns)
+          if (ok) ok = cuda_ok(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, ksmem),
+                               "adjoint shared memory attribute");
+      });
     }
     if (ok && cm.nt > 0) {
       a.ctrl = ctrl;
@@ -1420,8 +1468,11 @@ void backward_impl(const BackwardCall<T>& bc) {
             timed(KK_IMAGE, st, [&] { launch_tm_image<T>(kind, a.e_only != 0, a.acc64 != 0, st, b.a, tl.Ez, tg); });
           else
             timed(KK_IMAGE, st, [&] {
-              k_image<T><<<img_blocks, 256, 0, st>>>(b.a, kb.Ex, kb.Ey, kb.Ez, (long long)g.NX * g.NY * kg.zp,
-                                                     g.NY * kg.zp, kg.zp);
+              const long long ls = (long long)g.NX * g.NY * kg.zp;
+              if (a.box.cells() < (1LL << 31))
+                launch_k3_image<T>(kind, a.e_only != 0, a.acc64 != 0, cm.mode, st, b.a, kb, ls, g.NY * kg.zp, kg.zp);
+              else
+                k_image<T><<<img_blocks, 256, 0, st>>>(b.a, kb.Ex, kb.Ey, kb.Ez, ls, g.NY * kg.zp, kg.zp);
             });
         }
         if (tm2d) {
@@ -1459,28 +1510,17 @@ void backward_impl(const BackwardCall<T>& bc) {
           });
         } else {
           const unsigned nb = (unsigned)kg.nblocks;
-          const bool eq3 = cm.dy == cm.dx && cm.dz == cm.dx;
           timed(KK_ADJ_E, st, [&] {
-            if (eq3) {
-              if (R == 1) k3v_adj_e<T, 1, true><<<nb, kblock, ksmem, st>>>(b, kb, kg);
-              else if (R == 2) k3v_adj_e<T, 2, true><<<nb, kblock, ksmem, st>>>(b, kb, kg);
-              else k3v_adj_e<T, 4, true><<<nb, kblock, ksmem, st>>>(b, kb, kg);
-            } else {
-              if (R == 1) k3v_adj_e<T, 1, false><<<nb, kblock, ksmem, st>>>(b, kb, kg);
-              else if (R == 2) k3v_adj_e<T, 2, false><<<nb, kblock, ksmem, st>>>(b, kb, kg);
-              else k3v_adj_e<T, 4, false><<<nb, kblock, ksmem, st>>>(b, kb, kg);
-            }
+            k3_variant<T>(R, eq3, gen3, [&](auto RR, auto E, auto G) {
+              k3v_adj_e<T, decltype(RR)::value, decltype(E)::value, decltype(G)::value>
+                  <<<nb, kblock, ksmem, st>>>(b, kb, kg);
+            });
           });
           timed(KK_ADJ_H, st, [&] {
-            if (eq3) {
-              if (R == 1) k3v_adj_h<T, 1, true><<<nb, kblock, ksmem, st>>>(b, kb, kg);
-              else if (R == 2) k3v_adj_h<T, 2, true><<<nb, kblock, ksmem, st>>>(b, kb, kg);
-              else k3v_adj_h<T, 4, true><<<nb, kblock, ksmem, st>>>(b, kb, kg);
-            } else {
-              if (R == 1) k3v_adj_h<T, 1, false><<<nb, kblock, ksmem, st>>>(b, kb, kg);
-              else if (R == 2) k3v_adj_h<T, 2, false><<<nb, kblock, ksmem, st>>>(b, kb, kg);
-              else k3v_adj_h<T, 4, false><<<nb, kblock, ksmem, st>>>(b, kb, kg);
-            }
+            k3_variant<T>(R, eq3, gen3, [&](auto RR, auto E, auto G) {
+              k3v_adj_h<T, decltype(RR)::value, decltype(E)::value, decltype(G)::value>
+                  <<<nb, kblock, ksmem, st>>>(b, kb, kg);
+            });
           });
         }
       };
