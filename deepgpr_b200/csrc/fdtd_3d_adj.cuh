@@ -108,6 +108,15 @@ __device__ __forceinline__ long long cpml_at(const Grid& g, int axis, int slot, 
   return psi_index(d, axis, s, q, i, j, k);
 }
 
+// The same in 32-bit arithmetic: the staged (single-face) kernels run only
+// when every CPML array has fewer than 2^31 elements.
+template <bool EFACE>
+__device__ __forceinline__ int cpml_at32(const Grid& g, int axis, int slot, int p, int s, int q, int i, int j, int k) {
+  const PsiDims d = EFACE ? psi_dims_e(g, axis, slot, p) : psi_dims_h(g, axis, slot, p);
+  const int u = axis == 0 ? q : i, v = axis == 1 ? q : j, w = axis == 2 ? q : k;
+  return ((s * d.a + u) * d.b + v) * d.c + w;
+}
+
 // Adjoint CPML weight with psi already loaded: returns w, stores psi
 // (pml_weight of fdtd_adjoint.cuh).
 template <typename T>
@@ -184,8 +193,13 @@ __device__ __noinline__ void head_gen(const TiledAdj<T>& P, int st, int s, int i
   if (epml) e_pml_head(P.a, s, i, j, k, c, ex, ey, ez);
 }
 
-// stage slots of the adjoint kernels
-constexpr int kAdjSlots = 13;
+// stage slots of the adjoint kernels: 13 fixed ones, then w1, w2 of the
+// y-face weights of the 2R neighbour rows of the gathers along y
+constexpr int kAdjSlots0 = 13;
+template <int R>
+__host__ __device__ constexpr int adj_slots() {
+  return kAdjSlots0 + 4 * R;
+}
 enum : int {
   kStXw1 = 0, kStXw2 = 1,      // weights of the entering x plane's channels
   kStZw1 = 2, kStZw2 = 3,      // z-face weights of the lane's columns
@@ -193,12 +207,13 @@ enum : int {
   kStPy1 = 6, kStPy2 = 7,      //   y face
   kStPz1 = 8, kStPz2 = 9,      //   z face
   kStUp = 10,                  // rhs coefficient of the cell
-  kStHw1 = 11, kStHw2 = 12     // z-face weights of the halo column (cell 0)
+  kStHw1 = 11, kStHw2 = 12,    // z-face weights of the halo column (cell 0)
+  kStY = 13                    // row m: kStY + 2 m (w1), kStY + 2 m + 1 (w2)
 };
 // dynamic shared memory of k3v_adj_e / k3v_adj_h: two stages per warp
-template <typename T>
-constexpr int k3_adj_smem_bytes() {
-  return K3_WARPS * 2 * kAdjSlots * 2 * 32 * (int)sizeof(T);
+template <typename T, int R>
+__host__ __device__ constexpr int k3_adj_smem_bytes() {
+  return K3_WARPS * 2 * adj_slots<R>() * 2 * 32 * (int)sizeof(T);
 }
 
 // ---------------------------------------------------------------------------
@@ -297,8 +312,9 @@ __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 
   const bool any_ez = __any_sync(kFullMask, ezq[0] >= 0 || ezq[1] >= 0 || ehq >= 0);
   const bool any_hz = __any_sync(kFullMask, hzq[0] >= 0 || hzq[1] >= 0);
 
-  extern __shared__ __align__(16) unsigned char k3_adj_smem[];   // k3_adj_smem_bytes<T>()
-  T(*const sg)[kAdjSlots][2][32] = reinterpret_cast<T(*)[kAdjSlots][2][32]>(k3_adj_smem) + 2 * threadIdx.y;
+  constexpr int NSL = adj_slots<R>();
+  extern __shared__ __align__(16) unsigned char k3_adj_smem[];   // k3_adj_smem_bytes<T, R>()
+  T(*const sg)[NSL][2][32] = reinterpret_cast<T(*)[NSL][2][32]>(k3_adj_smem) + 2 * threadIdx.y;
   // stages the CPML operands of plane i into stage b (one commit group per plane)
   auto stage = [&](int i, int b) {
     if (cps) {
@@ -310,7 +326,25 @@ __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 
       face_q<false>(a.hF[0].p, a.hF[1].p, i, NX, qh0, qh1);
       const bool hx_on = qh0 >= 0 || qh1 >= 0;
       const bool il = i < NX - 1;
-      if (xin || hx_on || hy_on || any_ez || any_hz) {
+      if (xin || hx_on || hy_on || any_ez || any_hz || ymask) {
+        // E y-face weights of the neighbour rows (A_Y, C_Y sources)
+#pragma unroll
+        for (int d = -(R - 1); d <= R; ++d) {
+          const int m = d + R - 1;
+          if (!((ymask >> m) & 1u)) continue;
+          const int y = j + d;
+          int q0, q1;
+          face_q<true>(a.eF[2].p, a.eF[3].p, y, NY, q0, q1);
+          const bool lo = q0 >= 0;
+          const int q = lo ? q0 : q1, py = lo ? a.eF[2].p : a.eF[3].p;
+          const T* YW1 = lo ? a.eF[2].w1 : a.eF[3].w1;
+          const T* YW2 = lo ? a.eF[2].w2 : a.eF[3].w2;
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            if (il && kv[e]) cp_async(&sg[b][kStY + 2 * m][e][lane], YW1 + cpml_at32<true>(g, 1, 1, py, s, q, i, y, kof[e]));
+            if (kl[e]) cp_async(&sg[b][kStY + 2 * m + 1][e][lane], YW2 + cpml_at32<true>(g, 1, 2, py, s, q, i, y, kof[e]));
+          }
+        }
         const bool xlo = qa >= 0;
         const int qx = xlo ? qa : qb, px = xlo ? a.eF[0].p : a.eF[1].p;
         const T* XW1 = xlo ? a.eF[0].w1 : a.eF[1].w1;
@@ -323,45 +357,45 @@ __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
           const int k = kof[e];
-          if (xin && jl && kv[e]) cp_async(&sg[b][kStXw1][e][lane], XW1 + cpml_at<true>(g, 0, 1, px, s, qx, xi, j, k));
-          if (xin && kl[e]) cp_async(&sg[b][kStXw2][e][lane], XW2 + cpml_at<true>(g, 0, 2, px, s, qx, xi, j, k));
+          if (xin && jl && kv[e]) cp_async(&sg[b][kStXw1][e][lane], XW1 + cpml_at32<true>(g, 0, 1, px, s, qx, xi, j, k));
+          if (xin && kl[e]) cp_async(&sg[b][kStXw2][e][lane], XW2 + cpml_at32<true>(g, 0, 2, px, s, qx, xi, j, k));
           if (ezq[e] >= 0) {
             if (il)
               cp_async(&sg[b][kStZw1][e][lane],
-                       (ezlo ? a.eF[4].w1 : a.eF[5].w1) + cpml_at<true>(g, 2, 1, pez, s, ezq[e], i, j, k));
+                       (ezlo ? a.eF[4].w1 : a.eF[5].w1) + cpml_at32<true>(g, 2, 1, pez, s, ezq[e], i, j, k));
             if (jl)
               cp_async(&sg[b][kStZw2][e][lane],
-                       (ezlo ? a.eF[4].w2 : a.eF[5].w2) + cpml_at<true>(g, 2, 2, pez, s, ezq[e], i, j, k));
+                       (ezlo ? a.eF[4].w2 : a.eF[5].w2) + cpml_at32<true>(g, 2, 2, pez, s, ezq[e], i, j, k));
           }
           const bool hz_on = hzq[e] >= 0;
           if (kv[e] && (hx_on || hy_on || hz_on)) cp_async(&sg[b][kStUp][e][lane], f.ch_rhs + i * PS + row + e);
           if (hx_on) {
             T* P1 = hxlo ? a.hF[0].psi1 : a.hF[1].psi1;
             T* P2 = hxlo ? a.hF[0].psi2 : a.hF[1].psi2;
-            if (kl[e]) cp_async(&sg[b][kStPx1][e][lane], P1 + cpml_at<false>(g, 0, 1, phx, s, qhx, i, j, k));
-            if (kv[e] && jl) cp_async(&sg[b][kStPx2][e][lane], P2 + cpml_at<false>(g, 0, 2, phx, s, qhx, i, j, k));
+            if (kl[e]) cp_async(&sg[b][kStPx1][e][lane], P1 + cpml_at32<false>(g, 0, 1, phx, s, qhx, i, j, k));
+            if (kv[e] && jl) cp_async(&sg[b][kStPx2][e][lane], P2 + cpml_at32<false>(g, 0, 2, phx, s, qhx, i, j, k));
           }
           if (hy_on) {
             T* P1 = hylo ? a.hF[2].psi1 : a.hF[3].psi1;
             T* P2 = hylo ? a.hF[2].psi2 : a.hF[3].psi2;
-            if (kl[e]) cp_async(&sg[b][kStPy1][e][lane], P1 + cpml_at<false>(g, 1, 1, phy, s, qhy, i, j, k));
-            if (kv[e] && il) cp_async(&sg[b][kStPy2][e][lane], P2 + cpml_at<false>(g, 1, 2, phy, s, qhy, i, j, k));
+            if (kl[e]) cp_async(&sg[b][kStPy1][e][lane], P1 + cpml_at32<false>(g, 1, 1, phy, s, qhy, i, j, k));
+            if (kv[e] && il) cp_async(&sg[b][kStPy2][e][lane], P2 + cpml_at32<false>(g, 1, 2, phy, s, qhy, i, j, k));
           }
           if (hz_on) {
             T* P1 = hzlo ? a.hF[4].psi1 : a.hF[5].psi1;
             T* P2 = hzlo ? a.hF[4].psi2 : a.hF[5].psi2;
-            if (jl) cp_async(&sg[b][kStPz1][e][lane], P1 + cpml_at<false>(g, 2, 1, phz, s, hzq[e], i, j, k));
-            if (il) cp_async(&sg[b][kStPz2][e][lane], P2 + cpml_at<false>(g, 2, 2, phz, s, hzq[e], i, j, k));
+            if (jl) cp_async(&sg[b][kStPz1][e][lane], P1 + cpml_at32<false>(g, 2, 1, phz, s, hzq[e], i, j, k));
+            if (il) cp_async(&sg[b][kStPz2][e][lane], P2 + cpml_at32<false>(g, 2, 2, phz, s, hzq[e], i, j, k));
           }
         }
         if (ehq >= 0) {
           const int pe = ehlo ? a.eF[4].p : a.eF[5].p;
           if (il)
             cp_async(&sg[b][kStHw1][0][lane],
-                     (ehlo ? a.eF[4].w1 : a.eF[5].w1) + cpml_at<true>(g, 2, 1, pe, s, ehq, i, j, hk));
+                     (ehlo ? a.eF[4].w1 : a.eF[5].w1) + cpml_at32<true>(g, 2, 1, pe, s, ehq, i, j, hk));
           if (jl)
             cp_async(&sg[b][kStHw2][0][lane],
-                     (ehlo ? a.eF[4].w2 : a.eF[5].w2) + cpml_at<true>(g, 2, 2, pe, s, ehq, i, j, hk));
+                     (ehlo ? a.eF[4].w2 : a.eF[5].w2) + cpml_at32<true>(g, 2, 2, pe, s, ehq, i, j, hk));
         }
       }
     }
@@ -535,8 +569,13 @@ __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 
       for (int e = 0; e < 2; ++e) {
         T w1 = T(0), w2 = T(0);
         if ((ymask >> m) & 1u) {
-          if (il && kv[e]) w1 = pml_w_gen<T, true>(a.eF[2], a.eF[3], g, 1, 1, s, i, y, kof[e]);
-          if (kl[e]) w2 = pml_w_gen<T, true>(a.eF[2], a.eF[3], g, 1, 2, s, i, y, kof[e]);
+          if (cps) {
+            if (il && kv[e]) w1 += sg[b][kStY + 2 * m][e][lane];
+            if (kl[e]) w2 += sg[b][kStY + 2 * m + 1][e][lane];
+          } else if (GEN) {
+            if (il && kv[e]) w1 = pml_w_gen<T, true>(a.eF[2], a.eF[3], g, 1, 1, s, i, y, kof[e]);
+            if (kl[e]) w2 = pml_w_gen<T, true>(a.eF[2], a.eF[3], g, 1, 2, s, i, y, kof[e]);
+          }
         }
         const T cye = curl_y<EQ>(a, cv[e]);
         if (dxo && il && ym && km[e]) w1 += cye * lx[e];
@@ -584,11 +623,11 @@ __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 
             const int q = lo ? qh0 : qh1;
             const Prof<T> pr = prof(F, q);
             if (kl[e]) {
-              const long long pi = cpml_at<false>(g, 0, 1, F.p, s, q, i, j, k);
+              const long long pi = cpml_at32<false>(g, 0, 1, F.p, s, q, i, j, k);
               F.w1[pi] = pml_weight_v(hy[e], a.inv_dx, up, T(1), pr, sg[b][kStPx1][e][lane], &F.psi1[pi]);
             }
             if (jl) {
-              const long long pi = cpml_at<false>(g, 0, 2, F.p, s, q, i, j, k);
+              const long long pi = cpml_at32<false>(g, 0, 2, F.p, s, q, i, j, k);
               F.w2[pi] = pml_weight_v(hz[e], a.inv_dx, up, T(-1), pr, sg[b][kStPx2][e][lane], &F.psi2[pi]);
             }
           }
@@ -598,11 +637,11 @@ __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 
             const int q = lo ? qhy0 : qhy1;
             const Prof<T> pr = prof(F, q);
             if (kl[e]) {
-              const long long pi = cpml_at<false>(g, 1, 1, F.p, s, q, i, j, k);
+              const long long pi = cpml_at32<false>(g, 1, 1, F.p, s, q, i, j, k);
               F.w1[pi] = pml_weight_v(hx[e], a.inv_dy, up, T(-1), pr, sg[b][kStPy1][e][lane], &F.psi1[pi]);
             }
             if (il) {
-              const long long pi = cpml_at<false>(g, 1, 2, F.p, s, q, i, j, k);
+              const long long pi = cpml_at32<false>(g, 1, 2, F.p, s, q, i, j, k);
               F.w2[pi] = pml_weight_v(hz[e], a.inv_dy, up, T(1), pr, sg[b][kStPy2][e][lane], &F.psi2[pi]);
             }
           }
@@ -611,11 +650,11 @@ __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 
             const int q = hzq[e];
             const Prof<T> pr = prof(F, q);
             if (jl) {
-              const long long pi = cpml_at<false>(g, 2, 1, F.p, s, q, i, j, k);
+              const long long pi = cpml_at32<false>(g, 2, 1, F.p, s, q, i, j, k);
               F.w1[pi] = pml_weight_v(hx[e], a.inv_dz, up, T(1), pr, sg[b][kStPz1][e][lane], &F.psi1[pi]);
             }
             if (il) {
-              const long long pi = cpml_at<false>(g, 2, 2, F.p, s, q, i, j, k);
+              const long long pi = cpml_at32<false>(g, 2, 2, F.p, s, q, i, j, k);
               F.w2[pi] = pml_weight_v(hy[e], a.inv_dz, up, T(-1), pr, sg[b][kStPz2][e][lane], &F.psi2[pi]);
             }
           }
@@ -725,8 +764,9 @@ __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 
   const bool any_ez = __any_sync(kFullMask, ezq[0] >= 0 || ezq[1] >= 0);
   const bool heads = head >= 0;
 
-  extern __shared__ __align__(16) unsigned char k3_adj_smem[];   // k3_adj_smem_bytes<T>()
-  T(*const sg)[kAdjSlots][2][32] = reinterpret_cast<T(*)[kAdjSlots][2][32]>(k3_adj_smem) + 2 * threadIdx.y;
+  constexpr int NSL = adj_slots<R>();
+  extern __shared__ __align__(16) unsigned char k3_adj_smem[];   // k3_adj_smem_bytes<T, R>()
+  T(*const sg)[NSL][2][32] = reinterpret_cast<T(*)[NSL][2][32]>(k3_adj_smem) + 2 * threadIdx.y;
   auto stage = [&](int i, int b) {
     if (cps) {
       const int xi = i + R - 1;   // entering plane of the x channels
@@ -737,7 +777,25 @@ __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 
       if (heads) face_q<true>(a.eF[0].p, a.eF[1].p, i, NX, qe0, qe1);
       const bool ex_on = qe0 >= 0 || qe1 >= 0;
       const bool il = i < NX - 1;
-      if (xin || ex_on || (heads && (ey_on || any_ez)) || any_hz) {
+      if (xin || ex_on || (heads && (ey_on || any_ez)) || any_hz || ymask) {
+        // H y-face weights of the neighbour rows (A_Y, C_Y sources)
+#pragma unroll
+        for (int d = -R; d <= R - 1; ++d) {
+          const int m = d + R;
+          if (!((ymask >> m) & 1u)) continue;
+          const int y = j + d;
+          int q0, q1;
+          face_q<false>(a.hF[2].p, a.hF[3].p, y, NY, q0, q1);
+          const bool lo = q0 >= 0;
+          const int q = lo ? q0 : q1, py = lo ? a.hF[2].p : a.hF[3].p;
+          const T* YW1 = lo ? a.hF[2].w1 : a.hF[3].w1;
+          const T* YW2 = lo ? a.hF[2].w2 : a.hF[3].w2;
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            if (kl[e]) cp_async(&sg[b][kStY + 2 * m][e][lane], YW1 + cpml_at32<false>(g, 1, 1, py, s, q, i, y, kof[e]));
+            if (il && kv[e]) cp_async(&sg[b][kStY + 2 * m + 1][e][lane], YW2 + cpml_at32<false>(g, 1, 2, py, s, q, i, y, kof[e]));
+          }
+        }
         const bool xlo = qa >= 0;
         const int qx = xlo ? qa : qb, px = xlo ? a.hF[0].p : a.hF[1].p;
         const T* XW1 = xlo ? a.hF[0].w1 : a.hF[1].w1;
@@ -750,15 +808,15 @@ __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
           const int k = kof[e];
-          if (xin && kl[e]) cp_async(&sg[b][kStXw1][e][lane], XW1 + cpml_at<false>(g, 0, 1, px, s, qx, xi, j, k));
-          if (xin && jl && kv[e]) cp_async(&sg[b][kStXw2][e][lane], XW2 + cpml_at<false>(g, 0, 2, px, s, qx, xi, j, k));
+          if (xin && kl[e]) cp_async(&sg[b][kStXw1][e][lane], XW1 + cpml_at32<false>(g, 0, 1, px, s, qx, xi, j, k));
+          if (xin && jl && kv[e]) cp_async(&sg[b][kStXw2][e][lane], XW2 + cpml_at32<false>(g, 0, 2, px, s, qx, xi, j, k));
           if (hzq[e] >= 0) {
             if (jl)
               cp_async(&sg[b][kStZw1][e][lane],
-                       (hzlo ? a.hF[4].w1 : a.hF[5].w1) + cpml_at<false>(g, 2, 1, phz, s, hzq[e], i, j, k));
+                       (hzlo ? a.hF[4].w1 : a.hF[5].w1) + cpml_at32<false>(g, 2, 1, phz, s, hzq[e], i, j, k));
             if (il)
               cp_async(&sg[b][kStZw2][e][lane],
-                       (hzlo ? a.hF[4].w2 : a.hF[5].w2) + cpml_at<false>(g, 2, 2, phz, s, hzq[e], i, j, k));
+                       (hzlo ? a.hF[4].w2 : a.hF[5].w2) + cpml_at32<false>(g, 2, 2, phz, s, hzq[e], i, j, k));
           }
           if (!heads) continue;
           const bool ez_on = ezq[e] >= 0;
@@ -766,30 +824,30 @@ __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 
           if (ex_on) {
             T* P1 = exlo ? a.eF[0].psi1 : a.eF[1].psi1;
             T* P2 = exlo ? a.eF[0].psi2 : a.eF[1].psi2;
-            if (kv[e] && jl) cp_async(&sg[b][kStPx1][e][lane], P1 + cpml_at<true>(g, 0, 1, pex, s, qex, i, j, k));
-            if (kl[e]) cp_async(&sg[b][kStPx2][e][lane], P2 + cpml_at<true>(g, 0, 2, pex, s, qex, i, j, k));
+            if (kv[e] && jl) cp_async(&sg[b][kStPx1][e][lane], P1 + cpml_at32<true>(g, 0, 1, pex, s, qex, i, j, k));
+            if (kl[e]) cp_async(&sg[b][kStPx2][e][lane], P2 + cpml_at32<true>(g, 0, 2, pex, s, qex, i, j, k));
           }
           if (ey_on) {
             T* P1 = eylo ? a.eF[2].psi1 : a.eF[3].psi1;
             T* P2 = eylo ? a.eF[2].psi2 : a.eF[3].psi2;
-            if (kv[e] && il) cp_async(&sg[b][kStPy1][e][lane], P1 + cpml_at<true>(g, 1, 1, pey, s, qey, i, j, k));
-            if (kl[e]) cp_async(&sg[b][kStPy2][e][lane], P2 + cpml_at<true>(g, 1, 2, pey, s, qey, i, j, k));
+            if (kv[e] && il) cp_async(&sg[b][kStPy1][e][lane], P1 + cpml_at32<true>(g, 1, 1, pey, s, qey, i, j, k));
+            if (kl[e]) cp_async(&sg[b][kStPy2][e][lane], P2 + cpml_at32<true>(g, 1, 2, pey, s, qey, i, j, k));
           }
           if (ez_on) {
             T* P1 = ezlo ? a.eF[4].psi1 : a.eF[5].psi1;
             T* P2 = ezlo ? a.eF[4].psi2 : a.eF[5].psi2;
-            if (il) cp_async(&sg[b][kStPz1][e][lane], P1 + cpml_at<true>(g, 2, 1, pez, s, ezq[e], i, j, k));
-            if (jl) cp_async(&sg[b][kStPz2][e][lane], P2 + cpml_at<true>(g, 2, 2, pez, s, ezq[e], i, j, k));
+            if (il) cp_async(&sg[b][kStPz1][e][lane], P1 + cpml_at32<true>(g, 2, 1, pez, s, ezq[e], i, j, k));
+            if (jl) cp_async(&sg[b][kStPz2][e][lane], P2 + cpml_at32<true>(g, 2, 2, pez, s, ezq[e], i, j, k));
           }
         }
         if (hhq >= 0) {
           const int ph = hhlo ? a.hF[4].p : a.hF[5].p;
           if (jl)
             cp_async(&sg[b][kStHw1][0][lane],
-                     (hhlo ? a.hF[4].w1 : a.hF[5].w1) + cpml_at<false>(g, 2, 1, ph, s, hhq, i, j, hk));
+                     (hhlo ? a.hF[4].w1 : a.hF[5].w1) + cpml_at32<false>(g, 2, 1, ph, s, hhq, i, j, hk));
           if (il)
             cp_async(&sg[b][kStHw2][0][lane],
-                     (hhlo ? a.hF[4].w2 : a.hF[5].w2) + cpml_at<false>(g, 2, 2, ph, s, hhq, i, j, hk));
+                     (hhlo ? a.hF[4].w2 : a.hF[5].w2) + cpml_at32<false>(g, 2, 2, ph, s, hhq, i, j, hk));
         }
       }
     }
@@ -959,8 +1017,13 @@ __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 
       for (int e = 0; e < 2; ++e) {
         T w1 = T(0), w2 = T(0);
         if ((ymask >> m) & 1u) {
-          if (kl[e]) w1 = pml_w_gen<T, false>(a.hF[2], a.hF[3], g, 1, 1, s, i, y, kof[e]);
-          if (il && kv[e]) w2 = pml_w_gen<T, false>(a.hF[2], a.hF[3], g, 1, 2, s, i, y, kof[e]);
+          if (cps) {
+            if (kl[e]) w1 += sg[b][kStY + 2 * m][e][lane];
+            if (il && kv[e]) w2 += sg[b][kStY + 2 * m + 1][e][lane];
+          } else if (GEN) {
+            if (kl[e]) w1 = pml_w_gen<T, false>(a.hF[2], a.hF[3], g, 1, 1, s, i, y, kof[e]);
+            if (il && kv[e]) w2 = pml_w_gen<T, false>(a.hF[2], a.hF[3], g, 1, 2, s, i, y, kof[e]);
+          }
         }
         const T cye = curl_y<EQ>(a, cv[e]);
         if (hxo && im && yl && kl[e]) w1 += (-cye) * lx[e];
@@ -1010,11 +1073,11 @@ __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 
               const int q = lo ? qe0 : qe1;
               const Prof<T> pr = prof(F, q);
               if (jl) {
-                const long long pi = cpml_at<true>(g, 0, 1, F.p, s, q, i, j, k);
+                const long long pi = cpml_at32<true>(g, 0, 1, F.p, s, q, i, j, k);
                 F.w1[pi] = pml_weight_v(ey[e], a.inv_dx, up, T(-1), pr, sg[b][kStPx1][e][lane], &F.psi1[pi]);
               }
               if (kl[e]) {
-                const long long pi = cpml_at<true>(g, 0, 2, F.p, s, q, i, j, k);
+                const long long pi = cpml_at32<true>(g, 0, 2, F.p, s, q, i, j, k);
                 F.w2[pi] = pml_weight_v(ez[e], a.inv_dx, up, T(1), pr, sg[b][kStPx2][e][lane], &F.psi2[pi]);
               }
             }
@@ -1024,11 +1087,11 @@ __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 
               const int q = lo ? qey0 : qey1;
               const Prof<T> pr = prof(F, q);
               if (il) {
-                const long long pi = cpml_at<true>(g, 1, 1, F.p, s, q, i, j, k);
+                const long long pi = cpml_at32<true>(g, 1, 1, F.p, s, q, i, j, k);
                 F.w1[pi] = pml_weight_v(ex[e], a.inv_dy, up, T(1), pr, sg[b][kStPy1][e][lane], &F.psi1[pi]);
               }
               if (kl[e]) {
-                const long long pi = cpml_at<true>(g, 1, 2, F.p, s, q, i, j, k);
+                const long long pi = cpml_at32<true>(g, 1, 2, F.p, s, q, i, j, k);
                 F.w2[pi] = pml_weight_v(ez[e], a.inv_dy, up, T(-1), pr, sg[b][kStPy2][e][lane], &F.psi2[pi]);
               }
             }
@@ -1037,11 +1100,11 @@ __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 
               const int q = ezq[e];
               const Prof<T> pr = prof(F, q);
               if (il) {
-                const long long pi = cpml_at<true>(g, 2, 1, F.p, s, q, i, j, k);
+                const long long pi = cpml_at32<true>(g, 2, 1, F.p, s, q, i, j, k);
                 F.w1[pi] = pml_weight_v(ex[e], a.inv_dz, up, T(-1), pr, sg[b][kStPz1][e][lane], &F.psi1[pi]);
               }
               if (jl) {
-                const long long pi = cpml_at<true>(g, 2, 2, F.p, s, q, i, j, k);
+                const long long pi = cpml_at32<true>(g, 2, 2, F.p, s, q, i, j, k);
                 F.w2[pi] = pml_weight_v(ey[e], a.inv_dz, up, T(1), pr, sg[b][kStPz2][e][lane], &F.psi2[pi]);
               }
             }

@@ -608,6 +608,22 @@ void k3_variant(int R, bool eq, bool gen, F&& f) {
   }
 }
 
+template <bool EFIELD>
+void psi_counts(const Grid& g, const int* p, long long* out);
+
+// The 3D kernels' single-face CPML form: along every axis the two faces are
+// at least 4 cells apart (a lane's two cells, a row and a plane lie in one
+// face at most) and every CPML array is indexed in 32 bits.
+bool k3_cpml_single(const Grid& g, const int* p) {
+  if (g.NX < p[0] + p[1] + 4 || g.NY < p[2] + p[3] + 4 || g.NZ < p[4] + p[5] + 4) return false;
+  long long ce[12], ch[12];
+  psi_counts<true>(g, p, ce);
+  psi_counts<false>(g, p, ch);
+  for (int q = 0; q < 12; ++q)
+    if (ce[q] >= (1LL << 31) || ch[q] >= (1LL << 31)) return false;
+  return true;
+}
+
 K3Geom k3_layout(const Grid& g) {
   K3Geom kg;
   memset(&kg, 0, sizeof(kg));
@@ -1044,8 +1060,7 @@ void forward_impl(const ForwardCall<T>& fc) {
       kg = k3_layout(g);
       kg.src_rows = src_rows;
       kg.rcv_rows = rcv_rows;
-      const int* pf = cm.p;   // face thicknesses x0, xm, y0, ym, z0, zm
-      kg.cpml_single = g.NX >= pf[0] + pf[1] + 4 && g.NY >= pf[2] + pf[3] + 4 && g.NZ >= pf[4] + pf[5] + 4;
+      kg.cpml_single = k3_cpml_single(g, cm.p);
       ok = k3_alloc_pack(scratch, g, kg, cm, st, kf, fc.Ex, fc.Ey, fc.Ez, fc.Hx, fc.Hy, fc.Hz);
     }
     if (ok) {
@@ -1405,12 +1420,10 @@ void backward_impl(const BackwardCall<T>& bc) {
       kg = k3_layout(g);
       kg.src_rows = src_rows;
       kg.rcv_rows = rcv_rows;
-      const int* pf = cm.p;
-      kg.cpml_single = g.NX >= pf[0] + pf[1] + 4 && g.NY >= pf[2] + pf[3] + 4 && g.NZ >= pf[4] + pf[5] + 4;
+      kg.cpml_single = k3_cpml_single(g, cm.p);
       ok = k3_alloc_pack(scratch, g, kg, cm, st, kb, bc.lEx, bc.lEy, bc.lEz, bc.lHx, bc.lHy, bc.lHz);
     }
     const dim3 kblock(32, K3_WARPS);
-    const int ksmem = k3_adj_smem_bytes<T>();
     const bool eq3 = cm.dy == cm.dx && cm.dz == cm.dx;
     const bool gen3 = has_cpml && !kg.cpml_single;
     if (ok && !tm2d) {
@@ -1420,8 +1433,9 @@ void backward_impl(const BackwardCall<T>& bc) {
         constexpr bool e = decltype(E)::value, gn = decltype(G)::value;
         const void* fns[2] = {(const void*)k3v_adj_e<T, r, e, gn>, (const void*)k3v_adj_h<T, r, e, gn>};
         for (const void* fn : fns)
-          if (ok) ok = cuda_ok(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, ksmem),
-                               "adjoint shared memory attribute");
+          if (ok)
+            ok = cuda_ok(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, k3_adj_smem_bytes<T, r>()),
+                         "adjoint shared memory attribute");
       });
     }
     if (ok && cm.nt > 0) {
@@ -1512,14 +1526,16 @@ void backward_impl(const BackwardCall<T>& bc) {
           const unsigned nb = (unsigned)kg.nblocks;
           timed(KK_ADJ_E, st, [&] {
             k3_variant<T>(R, eq3, gen3, [&](auto RR, auto E, auto G) {
-              k3v_adj_e<T, decltype(RR)::value, decltype(E)::value, decltype(G)::value>
-                  <<<nb, kblock, ksmem, st>>>(b, kb, kg);
+              constexpr int r = decltype(RR)::value;
+              k3v_adj_e<T, r, decltype(E)::value, decltype(G)::value>
+                  <<<nb, kblock, k3_adj_smem_bytes<T, r>(), st>>>(b, kb, kg);
             });
           });
           timed(KK_ADJ_H, st, [&] {
             k3_variant<T>(R, eq3, gen3, [&](auto RR, auto E, auto G) {
-              k3v_adj_h<T, decltype(RR)::value, decltype(E)::value, decltype(G)::value>
-                  <<<nb, kblock, ksmem, st>>>(b, kb, kg);
+              constexpr int r = decltype(RR)::value;
+              k3v_adj_h<T, r, decltype(E)::value, decltype(G)::value>
+                  <<<nb, kblock, k3_adj_smem_bytes<T, r>(), st>>>(b, kb, kg);
             });
           });
         }
