@@ -15,6 +15,14 @@ than L2, so no flush is needed between steps.
 Multi-GPU (torchrun): every rank solves its own 32 shots (weak scaling) and
 the material gradient is summed with one NCCL all-reduce per step.
 
+The line also carries "north_star_3d": the 3D order-4 forward and adjoint
+on the 320 x 320 x 160 grid of the precision study (CPML 10 -> 340 x 340 x
+180 extended cells, gradient mode 3, FP32 E-only history, 32 x 32 receivers),
+on a bounded sample of 4 shots and 40 time steps, with the kernels' CUDA-event
+time split into forward (H, E) and adjoint (E, H, imaging) and their HBM
+roofline fractions at 72 B (forward + E history) and 104 B (adjoint) per
+cell-update.
+
 ``--impl reference`` times the reference's own C/OpenMP CPU backend
 (oracle/_ref, compiled from the reference source) on a bounded sample of the
 same workload with all host threads.
@@ -50,6 +58,10 @@ def parse():
     ap.add_argument("--shots", type=int, default=32)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-3d", action="store_true")
+    ap.add_argument("--only-3d", action="store_true", help="print the north_star_3d object alone (profiling)")
+    ap.add_argument("--nt-3d", type=int, default=40)
+    ap.add_argument("--shape-3d", default="320,320,160", help="physical grid of the 3D measurement")
     return ap.parse_args()
 
 
@@ -276,6 +288,10 @@ def ours(args, rank, world, local):
         "avg_launch_us": {k: round(v[0] / v[1] * 1e3, 2) for k, v in prof.items() if v[1]},
     }
 
+    ns3d = None
+    if rank == 0 and world == 1 and not args.no_3d:
+        ns3d = north_star_3d(dev, nt=args.nt_3d, shape=tuple(int(v) for v in args.shape_3d.split(",")))
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(args.shots, budget_s=15.0)
@@ -290,9 +306,70 @@ def ours(args, rank, world, local):
                        "fdtd_order": 4, "mode": 2, "history": "FP32 E-only (resident)",
                        "l2_policy": "inputs larger than L2 (132 MB fields, 132 GB history)"},
             "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-            "clocks": clocks.summary(), "loss": float(loss),
+            "clocks": clocks.summary(), "loss": float(loss), "north_star_3d": ns3d,
         }
         print(json.dumps(line), flush=True)
+
+
+# Algorithmic bytes per 3D cell-update (FP32): forward with E-only mode-3
+# history (E3, H3 rw + ce_hist, ce_curl, ch_curl + E^n), adjoint (lambda 6
+# components rw + 4 coefficients + E^n, E^(n+1) for 3 components + the
+# eps_r / sigma gradients rw).
+BYTES_PER_CELL_3D = {"forward": 72, "adjoint": 104}
+
+
+def north_star_3d(dev, shots=4, nt=40, warmup=1, steps=2, shape=(320, 320, 160)):
+    """3D order-4 forward + adjoint: kernel time split and HBM roofline fractions."""
+    import deepgpr_b200 as dg
+    from deepgpr_b200 import native
+    from deepgpr_b200.synthetic import fwi_3d
+
+    acq = fwi_3d(seed=1005, shape=shape, dx=0.015, sources_grid=(2, 2), receivers_grid=(32, 32), nt=nt, order=4)
+    common = dict(dx=acq.dx, dt=acq.dt, pmlthick=10, fdtd_order=4, mode=3)
+    src, rcv, wave = acq.sources.to(dev), acq.receivers.to(dev), acq.wavelet.to(dev)
+    eps0, sig0 = acq.eps_r.to(dev), acq.sigma.to(dev)
+
+    def gradient():
+        eps = eps0.clone().requires_grad_(True)
+        sig = sig0.clone().requires_grad_(True)
+        out = dg.compute(dev, source_amplitudes=wave, source_location=src, receiver_location=rcv, eps_r=eps,
+                         sigma=sig, **common)
+        loss = (out[-1] ** 2).sum()
+        del out
+        loss.backward()
+        return loss.detach()
+
+    for _ in range(warmup):
+        gradient()
+    torch.cuda.synchronize()
+    tot = {}
+    native.profile(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        gradient()
+    e1.record()
+    torch.cuda.synchronize()
+    prof = native.profile_read()
+    native.profile(False)
+    ext = tuple(n + 20 for n in shape)
+    cells = ext[0] * ext[1] * ext[2]
+    units = cells * nt * acq.sources.shape[0] * steps
+    peak, peak_kind = peaks()
+    fwd_ms = prof["fwd_h"][0] + prof["fwd_e"][0]
+    adj_ms = prof["adj_e"][0] + prof["adj_h"][0] + prof["image"][0]
+    fwd_rate, adj_rate = units / (fwd_ms / 1e3), units / (adj_ms / 1e3)
+    return {
+        "workload": f"3D order-4 forward + adjoint, {shape[0]}x{shape[1]}x{shape[2]} (ext {ext[0]}x{ext[1]}x{ext[2]}),"
+                    " mode 3, FP32 E-only history",
+        "sample": f"{acq.sources.shape[0]} shots x {nt} steps per gradient, {steps} gradients (of 16 shots x 3000)",
+        "forward_cell_updates_per_s": fwd_rate, "adjoint_cell_updates_per_s": adj_rate,
+        "gradient_cell_updates_per_s": 2 * units / (e0.elapsed_time(e1) / 1e3),
+        "forward_roofline_frac": round(fwd_rate * BYTES_PER_CELL_3D["forward"] / (peak * 1e9), 4),
+        "adjoint_roofline_frac": round(adj_rate * BYTES_PER_CELL_3D["adjoint"] / (peak * 1e9), 4),
+        "bytes_per_cell_update": BYTES_PER_CELL_3D, "peak_gbs": peak, "peak_source": peak_kind,
+        "kernel_ms_per_gradient": {k: round(v[0] / steps, 3) for k, v in prof.items() if v[1]},
+    }
 
 
 def cpu_baseline(shots: int, budget_s: float = 15.0, steps_hint: int = 0):
@@ -354,6 +431,10 @@ def main():
     try:
         if args.impl == "reference":
             reference(args, rank, world)
+        elif args.only_3d:
+            if rank == 0:
+                shape = tuple(int(v) for v in args.shape_3d.split(","))
+                print(json.dumps(north_star_3d(torch.device("cuda", local), nt=args.nt_3d, shape=shape)), flush=True)
         else:
             ours(args, rank, world, local)
     finally:
