@@ -23,6 +23,13 @@ time split into forward (H, E) and adjoint (E, H, imaging) and their HBM
 roofline fractions at 72 B (forward + E history) and 104 B (adjoint) per
 cell-update.
 
+"serving" (also in the line; ``--only-serving`` prints it alone): a seeded
+Poisson stream with config 4's request mix (nt scaled by 0.1, 40 requests,
+all arriving within ~0.6 s so both paths run at capacity) served by
+``deepgpr_b200.serving.SolveServer`` (8 slots, FP8 histories) and, for
+comparison, by plain per-request ``compute`` (+ ``backward``) calls one after
+another (FP32 histories); solves/s and p50/p99 latency of both.
+
 ``--impl reference`` times the reference's own C/OpenMP CPU backend
 (oracle/_ref, compiled from the reference source) on a bounded sample of the
 same workload with all host threads.
@@ -62,6 +69,9 @@ def parse():
     ap.add_argument("--only-3d", action="store_true", help="print the north_star_3d object alone (profiling)")
     ap.add_argument("--nt-3d", type=int, default=40)
     ap.add_argument("--shape-3d", default="320,320,160", help="physical grid of the 3D measurement")
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--only-serving", action="store_true", help="print the serving object alone")
+    ap.add_argument("--serving-requests", type=int, default=40)
     return ap.parse_args()
 
 
@@ -292,6 +302,18 @@ def ours(args, rank, world, local):
     if rank == 0 and world == 1 and not args.no_3d:
         ns3d = north_star_3d(dev, nt=args.nt_3d, shape=tuple(int(v) for v in args.shape_3d.split(",")))
 
+    serving = None
+    if rank == 0 and world == 1 and not args.no_serving:
+        # a serving process runs with PyTorch's stream-ordered allocator (see deepgpr_b200.serving)
+        env = dict(os.environ, PYTORCH_CUDA_ALLOC_CONF="backend:cudaMallocAsync")
+        cmd = [sys.executable, str(Path(__file__).resolve()), "--only-serving",
+               "--serving-requests", str(args.serving_requests)]
+        proc = subprocess.run(cmd, env=env, capture_output=True, text=True)
+        try:
+            serving = json.loads(proc.stdout.strip().splitlines()[-1])
+        except (IndexError, json.JSONDecodeError):
+            serving = {"error": (proc.stderr or proc.stdout)[-500:]}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(args.shots, budget_s=15.0)
@@ -306,7 +328,7 @@ def ours(args, rank, world, local):
                        "fdtd_order": 4, "mode": 2, "history": "FP32 E-only (resident)",
                        "l2_policy": "inputs larger than L2 (132 MB fields, 132 GB history)"},
             "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-            "clocks": clocks.summary(), "loss": float(loss), "north_star_3d": ns3d,
+            "clocks": clocks.summary(), "loss": float(loss), "north_star_3d": ns3d, "serving": serving,
         }
         print(json.dumps(line), flush=True)
 
@@ -372,6 +394,50 @@ def north_star_3d(dev, shots=4, nt=40, warmup=1, steps=2, shape=(320, 320, 160))
     }
 
 
+def serving_measure(dev, n=40, slots=8):
+    """Config-4 stream: continuous-batching server (FP8) vs plain per-request launches (FP32)."""
+    from deepgpr_b200.serving import SolveServer, percentile, run_plain
+    from deepgpr_b200.synthetic import serving_stream
+
+    reqs, arrivals = serving_stream(n=n)
+    warm, _ = serving_stream(seed=7, n=4, nt_scale=0.02)
+    run_plain(warm, dev)                                   # load, first-call set-up
+    torch.cuda.synchronize()
+    plain = run_plain(reqs, dev, arrivals=arrivals, history="fp32")
+    torch.cuda.synchronize()
+    with SolveServer(dev, slots=slots, history="fp8") as srv:
+        for f in [srv.submit(r) for r in warm]:
+            f.result()
+        t0 = time.perf_counter()
+        futs = []
+        for req, at in zip(reqs, arrivals):
+            wait = at - (time.perf_counter() - t0)
+            if wait > 0:
+                time.sleep(wait)
+            futs.append(srv.submit(req))
+        served = [f.result() for f in futs]
+        peak_running, peak_reserved = srv.peak_running, srv.peak_reserved
+
+    def summary(res):
+        span = max(r.finished for r in res) - min(r.submitted for r in res)
+        lat = [r.latency for r in res]
+        return {"solves_per_s": len(res) / span, "p50_latency_s": percentile(lat, 50),
+                "p99_latency_s": percentile(lat, 99), "span_s": span}
+
+    sp, ss = summary(plain), summary(served)
+    kinds = {k: sum(r.kind == k for r in reqs) for k in ("forward", "gradient")}
+    return {
+        "workload": "config-4 request mix (2D forward 128^2-1024^2 x 1-16 shots, order 2/4; 3D gradient "
+                    "96^3-160^3 x 1-4 shots, order 4), seeded Poisson arrivals",
+        "sample": f"{n} requests ({kinds['forward']} forward, {kinds['gradient']} gradient), nt scaled by 0.1, "
+                  f"arrivals within {arrivals[-1]:.2f} s",
+        "plain": dict(sp, history="fp32", path="compute (+ backward) per request, one after another"),
+        "served": dict(ss, history="fp8", slots=slots, peak_running=peak_running,
+                       peak_reserved_gib=round(peak_reserved / 2**30, 2)),
+        "speedup_solves_per_s": ss["solves_per_s"] / sp["solves_per_s"],
+    }
+
+
 def cpu_baseline(shots: int, budget_s: float = 15.0, steps_hint: int = 0):
     """Reference C/OpenMP backend (oracle/_ref) on a bounded sample: nt truncated."""
     from oracle import driver
@@ -431,6 +497,9 @@ def main():
     try:
         if args.impl == "reference":
             reference(args, rank, world)
+        elif args.only_serving:
+            if rank == 0:
+                print(json.dumps(serving_measure(torch.device("cuda", local), n=args.serving_requests)), flush=True)
         elif args.only_3d:
             if rank == 0:
                 shape = tuple(int(v) for v in args.shape_3d.split(","))

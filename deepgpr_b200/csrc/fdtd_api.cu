@@ -1745,6 +1745,24 @@ DGB_API int dgb_check_fixed_division(float divisor, unsigned long long* mismatch
   return 0;
 }
 
+// Scratch retention: the solver's per-call scratch comes from the current
+// device's default stream-ordered memory pool, which by default returns freed
+// memory to the system at every synchronisation.  A long-running caller that
+// solves back to back (a serving loop) keeps up to `bytes` cached in the pool
+// instead (-1: no limit); 0 restores the default and trims the pool.
+DGB_API int dgb_set_scratch_retention(long long bytes) {
+  int dev = 0;
+  if (!cuda_ok(cudaGetDevice(&dev), "dgb_set_scratch_retention: device")) return -1;
+  cudaMemPool_t pool;
+  if (!cuda_ok(cudaDeviceGetDefaultMemPool(&pool, dev), "dgb_set_scratch_retention: pool")) return -1;
+  unsigned long long v = bytes < 0 ? ~0ULL : (unsigned long long)bytes;   // the attribute is a 64-bit unsigned
+  if (!cuda_ok(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &v),
+               "dgb_set_scratch_retention: release threshold"))
+    return -1;
+  if (bytes == 0 && !cuda_ok(cudaMemPoolTrimTo(pool, 0), "dgb_set_scratch_retention: trim")) return -1;
+  return 0;
+}
+
 DGB_API int deepgpr_abi_version(void) { return 6; }
 DGB_API int deepgpr_supports_error_reporting(void) { return 1; }
 DGB_API const char* deepgpr_last_error(void) { return g_error; }

@@ -56,15 +56,21 @@ class ExtendIntoPML(torch.autograd.Function):
 
     @staticmethod
     def backward(ctx, grad: torch.Tensor):  # type: ignore[override]
-        for axis, n in enumerate(ctx.shape):
-            lo, hi = ctx.pml[2 * axis], ctx.pml[2 * axis + 1]
-            inner = grad.narrow(axis, lo, n).clone()
-            if lo:
-                inner.select(axis, 0).add_(grad.narrow(axis, 0, lo).sum(dim=axis))
-            if hi:
-                inner.select(axis, n - 1).add_(grad.narrow(axis, lo + n, hi).sum(dim=axis))
-            grad = inner
-        return grad.contiguous(), None
+        return fold_into_edges(grad, ctx.shape, ctx.pml), None
+
+
+def fold_into_edges(grad: torch.Tensor, shape: Sequence[int], pml: Sequence[int]) -> torch.Tensor:
+    """Adjoint of the replicate pad: CPML-slab gradients summed onto the edge cells,
+    one axis at a time (``_ExtendModel`` backward, ``model_setup.py:72-98``)."""
+    for axis, n in enumerate(shape):
+        lo, hi = int(pml[2 * axis]), int(pml[2 * axis + 1])
+        inner = grad.narrow(axis, lo, n).clone()
+        if lo:
+            inner.select(axis, 0).add_(grad.narrow(axis, 0, lo).sum(dim=axis))
+        if hi:
+            inner.select(axis, n - 1).add_(grad.narrow(axis, lo + n, hi).sum(dim=axis))
+        grad = inner
+    return grad.contiguous()
 
 
 def shift_locations(locations: torch.Tensor, pml: Sequence[int], device: Any) -> torch.Tensor:

@@ -103,6 +103,7 @@ SCALAR_SYMBOLS: Dict[str, Tuple[Tuple[str, ...], Optional[str]]] = {
     "dgb_set_options": (("int", "int", "int", "int"), "int"),
     "dgb_history_bytes": (("int", "int", "int", "int", "long long", "int", "int", "int", "int"), "long long"),
     "dgb_check_fixed_division": (("float", "void*", "void*"), "int"),
+    "dgb_set_scratch_retention": (("long long",), "int"),
     "dgb_profile": (("int",), None),
     "dgb_launch_count": ((), "long long"),
     "dgb_profile_read": (("void*", "void*", "int"), "int"),
@@ -129,6 +130,14 @@ def profile_read() -> Dict[str, Tuple[float, int]]:
     cnt = (ctypes.c_longlong * n)()
     lib.dgb_profile_read(ctypes.cast(ms, ctypes.c_void_p), ctypes.cast(cnt, ctypes.c_void_p), n)
     return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(KERNEL_KINDS)}
+
+def set_scratch_retention(nbytes: int) -> None:
+    """Keep up to ``nbytes`` of the solver's freed scratch cached on the current
+    device (-1: no limit, 0: the default, trimmed); see ``dgb_set_scratch_retention``."""
+    lib = load_library()
+    if lib.dgb_set_scratch_retention(int(nbytes)) != 0:
+        raise NativeLibraryError(last_error(lib) or "dgb_set_scratch_retention failed")
+
 
 def check_fixed_division(divisor: float) -> Tuple[int, int]:
     """(mismatches, lowest mismatching bit pattern) of the solver's division by

@@ -43,7 +43,7 @@ from .config import (
 )
 from .errors import NativeLibraryError, NonFiniteTensorError
 from .grid import normalize_grid_spacing, positive_finite
-from .model import prepare_model, shift_locations
+from .model import fold_into_edges, prepare_model, shift_locations
 from .pml import build_pml_coefficients, build_psi, face_descriptors
 from .storage import (
     StorageConfig,
@@ -321,7 +321,7 @@ def _alias(name: str, value: Any, alias: str, alias_value: Any) -> Any:
     return alias_value if value is None else value
 
 
-def compute(
+def _prepare_solve(
     device,
     dx=None,
     dt=None,
@@ -362,14 +362,8 @@ def compute(
     precision=torch.float32,
     gradient_accumulation="float64",
 ):
-    """2D/3D Maxwell FDTD forward modelling with an exact discrete adjoint on B200.
-
-    Arguments and return value are those of ``DeepGPR.compute``; see the module
-    docstring for the two additions (``wavefield_compression="fp8"``,
-    ``precision``) and ``gradient_accumulation`` (``"float64"``: the material
-    gradient is summed over shots and time in FP64; ``"float32"``: in FP32 in
-    the reference's order).
-    """
+    """Validation and preparation of ``compute``: the solver configuration, the
+    prepared tensors and model, and the 30 input states."""
     eps_r = _alias("eps_r", eps_r, "er", er)
     sigma = _alias("sigma", sigma, "se", se)
     mu_r = _alias("mu_r", mu_r, "mr", mr)
@@ -465,10 +459,107 @@ def compute(
         mu_r_pad=prepared.mu_r_pad.detach().contiguous(), source_location=src_loc, receiver_location=rcv_loc,
         pml_coefficients=tuple(c.contiguous() for c in coefficients),
     )
+    return cfg, tensors, prepared, (*electric, *magnetic, *psi)
+
+
+def compute(
+    device,
+    dx=None,
+    dt=None,
+    source_amplitudes=None,
+    source_location=None,
+    receiver_location=None,
+    er=None,
+    se=None,
+    mr=None,
+    E=None,
+    H=None,
+    PML=None,
+    pmlthick=DEFAULT_PML_THICKNESS,
+    source_direction=DEFAULT_SOURCE_COMPONENT,
+    reciever_direction=DEFAULT_RECEIVER_COMPONENT,
+    model_gradient_sampling_interval=DEFAULT_SAMPLING_INTERVAL,
+    wavefield_storage_dtype=torch.float32,
+    use_async_offload=False,
+    fdtd_order=DEFAULT_FDTD_ORDER,
+    mode=DEFAULT_GRADIENT_MODE,
+    debug=False,
+    print_parameters=False,
+    save_forward_wavefield_path=None,
+    *,
+    eps_r=None,
+    sigma=None,
+    mu_r=None,
+    receiver_component=None,
+    save_wavefield_history=True,
+    wavefield_compression="none",
+    wavefield_compression_block_size=None,
+    wavefield_conversion_backend="auto",
+    int8_reduction_backend="auto",
+    wavefield_compression_rate=None,
+    wavefield_rhs_history="auto",
+    wavefield_history_region="extended",
+    pml_max_velocity=SPEED_OF_LIGHT,
+    precision=torch.float32,
+    gradient_accumulation="float64",
+):
+    """2D/3D Maxwell FDTD forward modelling with an exact discrete adjoint on B200.
+
+    Arguments and return value are those of ``DeepGPR.compute``; see the module
+    docstring for the two additions (``wavefield_compression="fp8"``,
+    ``precision``) and ``gradient_accumulation`` (``"float64"``: the material
+    gradient is summed over shots and time in FP64; ``"float32"``: in FP32 in
+    the reference's order).
+    """
+    cfg, tensors, prepared, states_in = _prepare_solve(**locals())
     outputs = FDTDFunction.apply(cfg, tensors, prepared.eps_r, prepared.sigma, prepared.source_amplitudes,
-                                 *electric, *magnetic, *psi)
+                                 *states_in)
     states, e_saved, receivers = outputs[:STATE_COUNT], outputs[STATE_COUNT], outputs[STATE_COUNT + 1]
     return e_saved, tuple(states[0:3]), tuple(states[3:6]), tuple(states[6:30]), receivers
+
+
+class _DirectContext:
+    """The autograd context's part that FDTDFunction uses, for calls made
+    directly on the calling thread."""
+
+    def __init__(self, needs_input_grad):
+        self.needs_input_grad = needs_input_grad
+
+    def set_materialize_grads(self, value):
+        pass
+
+    def mark_non_differentiable(self, *tensors):
+        pass
+
+
+def misfit_gradient(device, observed, **kwargs):
+    """L2-misfit gradient of one solve, forward and adjoint run on the calling thread.
+
+    Takes ``compute``'s arguments (keywords, ``eps_r`` and ``sigma`` required)
+    and ``observed`` receiver data shaped like ``compute``'s receivers.
+    Returns ``(loss, grad_eps_r, grad_sigma, receivers)``: the gradients of
+    ``0.5 * sum((receivers - observed) ** 2)`` with respect to the physical
+    ``eps_r`` and ``sigma``, the values ``loss.backward()`` after ``compute``
+    gives.  The native adjoint is called from this thread instead of the
+    autograd engine's single per-device thread, so gradient solves issued by
+    several threads (each on its own CUDA stream) overlap on the GPU.
+    """
+    eps = kwargs.pop("eps_r").detach().requires_grad_(True)
+    sig = kwargs.pop("sigma").detach().requires_grad_(True)
+    cfg, tensors, prepared, states = _prepare_solve(device=device, eps_r=eps, sigma=sig, **kwargs)
+    ctx = _DirectContext((False, False, True, True, False) + (False,) * STATE_COUNT)
+    with torch.no_grad():
+        outs = FDTDFunction.forward(ctx, cfg, tensors, prepared.eps_r, prepared.sigma, prepared.source_amplitudes,
+                                    *states)
+        receivers = outs[STATE_COUNT + 1]
+        resid = receivers - observed.to(device=receivers.device, dtype=receivers.dtype)
+        loss = 0.5 * (resid * resid).sum()
+        grads = FDTDFunction.backward(ctx, *([None] * (STATE_COUNT + 1)), resid)
+        pml = prepared.pml
+        phys = tuple(n - pml[2 * a] - pml[2 * a + 1] for a, n in enumerate(prepared.eps_r.shape))
+        g_eps = fold_into_edges(grads[2], phys, pml).reshape(eps.shape)
+        g_sig = fold_into_edges(grads[3], phys, pml).reshape(sig.shape)
+    return loss, g_eps, g_sig, receivers
 
 
 def checkpoint_initial_field(device=None, per_nstep=None, dx=None, dt=None, source_amplitudes=None,

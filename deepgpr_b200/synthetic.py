@@ -117,3 +117,54 @@ def fwi_3d(seed: int = 1003, shape=(200, 200, 200), dx=0.02, sources_grid=(2, 4)
     ext = tuple(n + 20 for n in shape)
     dt = 0.9 * max_stable_time_step(dx, *ext, fdtd_order=order)
     return Acquisition(eps, sig, eps.clone(), src, rcv, ricker(freq, nt, dt)[None], dx, dt, order, 3)
+
+
+def serving_stream(seed: int = 1004, n: int = 40, nt_scale: float = 0.1, mean_gap_s: float = 0.01):
+    """Config-4 request stream: seeded Poisson arrivals, 70 % 2D forward solves
+    (square grids log-uniform in [128, 1024]^2, nt in [1000, 4000], 1-16 shots,
+    order 2 or 4) and 30 % 3D gradient solves (cubic grids log-uniform in
+    [96, 160]^3, nt in [800, 1500], 1-4 shots, order 4), models drawn as in
+    configs 2 and 3, Ricker 150-500 MHz.  ``nt_scale`` shortens every nt (a
+    bounded sample of the stream); gradient requests use zero observed data
+    (misfit = receiver energy).  Returns ``(requests, arrival_seconds)``.
+    """
+    import math
+
+    from .serving import SolveRequest
+
+    gen = torch.Generator().manual_seed(seed)
+
+    def uni(a, b):
+        return a + (b - a) * float(torch.rand((), generator=gen))
+
+    def loguni(a, b):
+        return int(round(math.exp(uni(math.log(a), math.log(b)))))
+
+    reqs, arrivals, t = [], [], 0.0
+    for k in range(n):
+        t += -mean_gap_s * math.log(max(1e-12, 1.0 - float(torch.rand((), generator=gen))))
+        freq = uni(150e6, 500e6)
+        if float(torch.rand((), generator=gen)) < 0.7:
+            size = loguni(128, 1024)
+            nt = max(16, int(uni(1000, 4000) * nt_scale))
+            shots = int(uni(1, 17))
+            order = 2 if float(torch.rand((), generator=gen)) < 0.5 else 4
+            acq = fwi_2d(seed=seed * 1000 + k, shape=(size, size), nshot=shots, nrx=min(64, size), nt=nt,
+                         freq=freq, order=order, air_rows=min(20, size // 8))
+            reqs.append(SolveRequest(kind="forward", eps_r=acq.eps_r, sigma=acq.sigma,
+                                     source_amplitudes=acq.wavelet, source_location=acq.sources,
+                                     receiver_location=acq.receivers, dx=acq.dx, dt=acq.dt, pmlthick=10,
+                                     fdtd_order=order, mode=2, tag=f"2d-fwd-{k}"))
+        else:
+            size = loguni(96, 160)
+            nt = max(16, int(uni(800, 1500) * nt_scale))
+            shots = int(uni(1, 5))
+            acq = fwi_3d(seed=seed * 1000 + k, shape=(size, size, size), dx=0.02, sources_grid=(1, shots),
+                         receivers_grid=(8, 8), nt=nt, freq=freq, order=4)
+            obs = torch.zeros((shots, nt, acq.receivers.shape[1]))
+            reqs.append(SolveRequest(kind="gradient", eps_r=acq.eps_r, sigma=acq.sigma,
+                                     source_amplitudes=acq.wavelet, source_location=acq.sources,
+                                     receiver_location=acq.receivers, dx=acq.dx, dt=acq.dt, pmlthick=10,
+                                     fdtd_order=4, mode=3, observed=obs, tag=f"3d-grad-{k}"))
+        arrivals.append(t)
+    return reqs, arrivals

@@ -184,6 +184,16 @@ void dgb_forward_noalloc(
  * Synchronous; returns 0, or -1 with deepgpr_last_error() set. */
 int dgb_check_fixed_division(float divisor, unsigned long long* mismatches, unsigned* first_bad);
 
+/* No counterpart in the reference.  The solver's per-call device scratch
+ * (working copies, point tables, CPML weights) comes from the current device's
+ * default stream-ordered memory pool, which by default gives freed memory
+ * back at every synchronisation, so every call maps its scratch again.  A
+ * caller that solves back to back -- a serving loop -- keeps up to `bytes`
+ * cached in the pool (-1: no limit); 0 restores the default and trims the
+ * pool.  Affects every stream-ordered allocation of the process on that
+ * device.  Returns 0, or -1 with deepgpr_last_error() set. */
+int dgb_set_scratch_retention(long long bytes);
+
 /* Process-wide kernel timing (CUDA events around every time-step
  * kernel; graph replay is off while enabled).  dgb_profile(1) clears the
  * totals; dgb_profile_read fills ms[k] and launches[k] for the kinds

@@ -1,0 +1,218 @@
+"""Serving loop: admission by footprint and continuous batching.
+
+The CPU tests drive the admission logic with a stand-in solve; the GPU tests
+check that every result is the same alone and in a mix of concurrent requests,
+that the direct gradient path equals compute + backward, and the FP8-history
+gradient error against an FP64 run.
+"""
+
+from __future__ import annotations
+
+import threading
+import time
+
+import pytest
+import torch
+
+from deepgpr_b200.serving import SolveRequest, SolveResult, SolveServer, footprint_bytes, percentile
+
+
+def _req(tag, kind="forward", shape=(40, 60), shots=1, nt=50):
+    return SolveRequest(kind=kind, eps_r=torch.ones(shape), sigma=torch.zeros(shape),
+                        source_amplitudes=torch.zeros(1, nt),
+                        source_location=torch.zeros(shots, 1, 3, dtype=torch.int32),
+                        receiver_location=torch.zeros(shots, 4, 3, dtype=torch.int32), dx=0.01, dt=1e-11,
+                        tag=tag)
+
+
+def test_footprint_grows_with_work_and_fp8_is_smaller():
+    small = footprint_bytes(_req("a", "gradient", nt=100))
+    assert footprint_bytes(_req("b", "gradient", nt=400)) > small
+    assert footprint_bytes(_req("c", "gradient", nt=100, shots=4)) > small
+    assert footprint_bytes(_req("d", "forward", nt=100)) < small
+    big = _req("e", "gradient", shape=(100, 100, 100), nt=500)
+    assert footprint_bytes(big, "fp8") < footprint_bytes(big, "fp32")
+
+
+def test_percentile_nearest_rank():
+    v = [5.0, 1.0, 3.0, 2.0, 4.0]
+    assert percentile(v, 50) == 3.0
+    assert percentile(v, 99) == 5.0
+    assert percentile(v, 0) == 1.0
+
+
+def test_admission_respects_budget_and_arrival_order():
+    sizes = {f"r{i}": s for i, s in enumerate([40, 30, 50, 20, 60, 10, 30, 40])}
+    live = []
+    lock = threading.Lock()
+    order = []
+
+    def run(req, slot):
+        with lock:
+            live.append(sizes[req.tag])
+            order.append(req.tag)
+            assert sum(live) <= 100
+        time.sleep(0.02)
+        with lock:
+            live.remove(sizes[req.tag])
+        return SolveResult(tag=req.tag, kind=req.kind)
+
+    server = SolveServer(slots=4, memory_budget=100, run=run, footprint=lambda r: sizes[r.tag])
+    futs = [server.submit(_req(t)) for t in sizes]
+    results = [f.result(timeout=10) for f in futs]
+    server.close()
+    assert [r.tag for r in results] == list(sizes)
+    assert server.admitted == list(sizes)    # admitted strictly in arrival order
+    assert sorted(order) == sorted(sizes)
+    assert server.peak_reserved <= 100
+    assert server.peak_running >= 2          # requests overlapped
+    st = server.stats()
+    assert st["solves"] == len(sizes) and st["p99_latency_s"] >= st["p50_latency_s"]
+
+
+def test_oversized_request_is_rejected_and_failures_do_not_stop_a_slot():
+    def run(req, slot):
+        if req.tag == "bad":
+            raise RuntimeError("solve failed")
+        return SolveResult(tag=req.tag, kind=req.kind)
+
+    server = SolveServer(slots=1, memory_budget=100, run=run,
+                         footprint=lambda r: 500 if r.tag == "huge" else 10)
+    huge = server.submit(_req("huge"))
+    with pytest.raises(MemoryError):
+        huge.result(timeout=5)
+    bad = server.submit(_req("bad"))
+    good = server.submit(_req("good"))
+    with pytest.raises(RuntimeError):
+        bad.result(timeout=5)
+    assert good.result(timeout=5).tag == "good"
+    server.close()
+
+
+def test_requests_wait_for_memory_released_by_finished_ones():
+    gate = threading.Event()
+    started = []
+
+    def run(req, slot):
+        started.append(req.tag)
+        if req.tag == "first":
+            gate.wait(5)
+        return SolveResult(tag=req.tag, kind=req.kind)
+
+    server = SolveServer(slots=2, memory_budget=100, run=run, footprint=lambda r: 60)
+    f1 = server.submit(_req("first"))
+    f2 = server.submit(_req("second"))
+    time.sleep(0.1)
+    assert started == ["first"]            # a slot is free, but memory is not
+    gate.set()
+    f1.result(timeout=5)
+    f2.result(timeout=5)
+    assert started == ["first", "second"]
+    server.close()
+
+
+# --------------------------------------------------------------------------- GPU
+
+
+def _problem(dims, kind, seed, nt, shots=1, order=4):
+    from deepgpr_b200.synthetic import ricker
+
+    g = torch.Generator().manual_seed(seed)
+    if dims == 2:
+        shape = (48 + 8 * seed, 64)
+        dx, dt, mode = 0.01, 1.5e-11, 2
+        src = torch.tensor([[[10, 10 + 12 * s, 0]] for s in range(shots)], dtype=torch.int32)
+        rcv = torch.tensor([[[8, j, 0] for j in range(4, 60, 8)]] * shots, dtype=torch.int32)
+    else:
+        shape = (20 + 2 * seed, 22, 18)
+        dx, dt, mode = 0.02, 1.5e-11, 3
+        src = torch.tensor([[[6, 6 + 4 * s, 8]] for s in range(shots)], dtype=torch.int32)
+        rcv = torch.tensor([[[4, j, 9] for j in range(2, 20, 4)]] * shots, dtype=torch.int32)
+    eps = 3.0 + 2.0 * torch.rand(shape, generator=g)
+    sig = 2e-3 * torch.rand(shape, generator=g)
+    wave = ricker(400e6, nt, dt)[None]
+    req = SolveRequest(kind=kind, eps_r=eps, sigma=sig, source_amplitudes=wave, source_location=src,
+                       receiver_location=rcv, dx=dx, dt=dt, pmlthick=6, fdtd_order=order, mode=mode,
+                       tag=f"{dims}d-{kind}-{seed}")
+    if kind == "gradient":
+        import deepgpr_b200 as dg
+
+        dev = torch.device("cuda", 0)
+        with torch.no_grad():
+            req.observed = dg.compute(dev, eps_r=(eps * 1.05).to(dev), sigma=sig.to(dev), source_amplitudes=wave.to(dev),
+                                      source_location=src.to(dev), receiver_location=rcv.to(dev), dx=dx, dt=dt,
+                                      pmlthick=6, fdtd_order=order, mode=mode,
+                                      save_wavefield_history=False)[-1].cpu()
+    return req
+
+
+def _same(a, b):
+    for name in ("receivers", "grad_eps_r", "grad_sigma"):
+        x, y = getattr(a, name), getattr(b, name)
+        assert (x is None) == (y is None), name
+        if x is not None:
+            assert torch.equal(x, y), name
+    if a.loss is not None:
+        assert a.loss == b.loss
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dims", [2, 3])
+def test_direct_gradient_equals_compute_backward(dims, cuda_device):
+    from deepgpr_b200.serving import run_plain
+    from deepgpr_b200.solver import misfit_gradient
+
+    req = _problem(dims, "gradient", 1, nt=60, shots=2)
+    plain = run_plain([req], cuda_device)[0]
+    kw = dict(dx=req.dx, dt=req.dt, pmlthick=req.pmlthick, fdtd_order=req.fdtd_order, mode=req.mode,
+              source_amplitudes=req.source_amplitudes.to(cuda_device),
+              source_location=req.source_location.to(cuda_device),
+              receiver_location=req.receiver_location.to(cuda_device))
+    loss, ge, gs, _ = misfit_gradient(cuda_device, req.observed.to(cuda_device), eps_r=req.eps_r.to(cuda_device),
+                                      sigma=req.sigma.to(cuda_device), **kw)
+    assert float(loss) == plain.loss
+    assert torch.equal(ge.cpu(), plain.grad_eps_r)
+    assert torch.equal(gs.cpu(), plain.grad_sigma)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("history", ["fp8", "fp32"])
+def test_results_are_the_same_alone_and_in_the_mix(history, cuda_device):
+    reqs = [_problem(2, "forward", 0, nt=80, shots=2), _problem(2, "gradient", 1, nt=80, shots=2),
+            _problem(3, "gradient", 2, nt=40), _problem(3, "forward", 3, nt=40, shots=2),
+            _problem(2, "gradient", 4, nt=70, order=2), _problem(3, "gradient", 5, nt=30, shots=2)]
+    alone = []
+    with SolveServer(cuda_device, slots=1, history=history) as one:
+        for r in reqs:
+            alone.append(one.submit(r).result(timeout=300))
+    with SolveServer(cuda_device, slots=4, history=history) as many:
+        futs = [many.submit(r) for r in reqs]
+        mixed = [f.result(timeout=300) for f in futs]
+        assert many.peak_running >= 2
+    for a, b in zip(alone, mixed):
+        _same(a, b)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dims", [2, 3])
+def test_fp8_served_gradient_error_against_fp64(dims, cuda_device):
+    """Served FP8-history gradient against an FP64 run of the same request (bound written here)."""
+    import deepgpr_b200 as dg
+    from helpers import rel_l2
+
+    req = _problem(dims, "gradient", 6, nt=120 if dims == 2 else 60, shots=2)
+    with SolveServer(cuda_device, slots=2, history="fp8") as srv:
+        got = srv.submit(req).result(timeout=300)
+    dev = cuda_device
+    eps = req.eps_r.to(dev, torch.float64).requires_grad_(True)
+    sig = req.sigma.to(dev, torch.float64).requires_grad_(True)
+    rx = dg.compute(dev, eps_r=eps, sigma=sig, source_amplitudes=req.source_amplitudes.to(dev, torch.float64),
+                    source_location=req.source_location.to(dev), receiver_location=req.receiver_location.to(dev),
+                    dx=req.dx, dt=req.dt, pmlthick=req.pmlthick, fdtd_order=req.fdtd_order, mode=req.mode,
+                    precision=torch.float64)[-1]
+    loss = 0.5 * ((rx - req.observed.to(dev, torch.float64)) ** 2).sum()
+    loss.backward()
+    e_eps = rel_l2(got.grad_eps_r, eps.grad)
+    e_sig = rel_l2(got.grad_sigma, sig.grad)
+    print(f"fp8 vs fp64 ({dims}D): grad_eps {e_eps:.3e}, grad_sigma {e_sig:.3e}")
+    assert e_eps < 2e-2 and e_sig < 2e-2
