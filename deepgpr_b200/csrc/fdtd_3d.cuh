@@ -30,6 +30,12 @@ namespace dg {
 
 constexpr int K3W = 64;       // z columns per warp strip (two per lane)
 constexpr int K3_WARPS = 4;   // warps (y rows) per CTA
+// Resident CTAs per SM the 3D kernels are built for: 12 warps per SM in FP32
+// at radius <= 2 (<= 168 registers a thread), 8 otherwise.
+template <typename T, int R>
+__host__ __device__ constexpr int k3_min_blocks() {
+  return (((R >= 4 || sizeof(T) == 8) ? 8 : 12) + K3_WARPS - 1) / K3_WARPS;
+}
 
 struct K3Geom {
   int zp;                          // z pitch of the working copy (multiple of 32)
@@ -285,7 +291,7 @@ constexpr int kStageSlots = 7;
 // 3D H half step (+ E^n history).  EQ: dx == dy == dz (curl scale 1).
 // ---------------------------------------------------------------------------
 template <typename T, int R, bool EQ, bool GEN>
-__global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 : 3) k3v_fwd_h(TiledFwd<T> P, K3Buf<T> f, K3Geom kg) {
+__global__ void __launch_bounds__(32 * K3_WARPS, k3_min_blocks<T, R>()) k3v_fwd_h(TiledFwd<T> P, K3Buf<T> f, K3Geom kg) {
   constexpr int ZLO = -(R - 1), ZHI = R + 1, NZN = ZHI - ZLO + 1;   // z neighbours of the pair, dfwd
   const FwdArgs<T>& a = P.a;
   const Grid& g = a.g;
@@ -637,7 +643,7 @@ __global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 
 // 3D E half step (+ sources, R^n history, receivers).
 // ---------------------------------------------------------------------------
 template <typename T, int R, bool EQ, bool GEN>
-__global__ void __launch_bounds__(32 * K3_WARPS, (R >= 4 || sizeof(T) == 8) ? 2 : 3) k3v_fwd_e(TiledFwd<T> P, K3Buf<T> f, K3Geom kg) {
+__global__ void __launch_bounds__(32 * K3_WARPS, k3_min_blocks<T, R>()) k3v_fwd_e(TiledFwd<T> P, K3Buf<T> f, K3Geom kg) {
   constexpr int ZLO = -R, ZHI = R, NZN = ZHI - ZLO + 1;   // z neighbours of the pair, dback
   const FwdArgs<T>& a = P.a;
   const Grid& g = a.g;
