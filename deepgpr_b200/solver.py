@@ -20,6 +20,7 @@ from __future__ import annotations
 import math
 import warnings
 from dataclasses import dataclass
+from datetime import datetime
 from typing import Any, Dict, Optional, Sequence, Tuple
 
 import torch
@@ -43,6 +44,7 @@ from .config import (
 )
 from .errors import NativeLibraryError, NonFiniteTensorError
 from .grid import normalize_grid_spacing, positive_finite
+from .history_io import normalize_forward_wavefield_directory, save_forward_wavefield
 from .model import fold_into_edges, prepare_model, shift_locations
 from .pml import build_pml_coefficients, build_psi, face_descriptors
 from .storage import (
@@ -404,8 +406,8 @@ def _prepare_solve(
         raise ValueError("use_async_offload=True is incompatible with save_wavefield_history=False.")
     if use_async_offload and compression == "fp8":
         raise ValueError("use_async_offload=True is incompatible with device-resident FP8 histories.")
-    if save_forward_wavefield_path is not None:
-        raise NotImplementedError("save_forward_wavefield_path: write E_saved with torch.save instead.")
+    if save_forward_wavefield_path is not None and not save_wavefield_history:
+        raise ValueError("save_forward_wavefield_path requires save_wavefield_history=True.")
     rhs_mode = normalize_choice("wavefield_rhs_history", wavefield_rhs_history, ("auto", "stored", "reconstructed"))
     region = normalize_choice("wavefield_history_region", wavefield_history_region, ("extended", "physical"))
     if source_direction not in FIELD_COMPONENTS or receiver_component not in FIELD_COMPONENTS:
@@ -511,10 +513,26 @@ def compute(
     gradient is summed over shots and time in FP64; ``"float32"``: in FP32 in
     the reference's order).
     """
-    cfg, tensors, prepared, states_in = _prepare_solve(**locals())
+    args = dict(locals())
+    output_directory = normalize_forward_wavefield_directory(save_forward_wavefield_path)
+    run_time = datetime.now() if output_directory is not None else None
+    cfg, tensors, prepared, states_in = _prepare_solve(**args)
     outputs = FDTDFunction.apply(cfg, tensors, prepared.eps_r, prepared.sigma, prepared.source_amplitudes,
                                  *states_in)
     states, e_saved, receivers = outputs[:STATE_COUNT], outputs[STATE_COUNT], outputs[STATE_COUNT + 1]
+    if output_directory is not None:
+        # reference file scheme (solver/modeling.py:640-663)
+        origin, cells = history_box(cfg.nx, cfg.ny, cfg.nz, cfg.pml, cfg.region)
+        shape = saved_history_shape(cfg.mode, saved_time_steps(cfg.nt, cfg.interval), cfg.nstep, *cells)
+        metadata = None
+        if cfg.storage.compression == "fp8":
+            metadata = {"compression": "fp8", "uncompressed_shape": shape, "field_shape": cfg.field_shape,
+                        "history_origin": origin, "tm2d": cfg.tm2d}
+        if cfg.region == "physical":
+            metadata = dict(metadata or {})
+            metadata.update(history_region="physical", history_origin=origin, pmlthick=cfg.pml,
+                            uncompressed_shape=shape)
+        save_forward_wavefield(e_saved, output_directory, run_time, metadata=metadata)
     return e_saved, tuple(states[0:3]), tuple(states[3:6]), tuple(states[6:30]), receivers
 
 

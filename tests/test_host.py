@@ -135,3 +135,24 @@ def test_checkpoint_initial_field_shapes():
     assert len(P) == 24
     assert P[0].shape == (1, 3, 20, 2)      # x0 E psi1: (nstep, p+1, ny, nz+1)
     assert P[16].numel() == 0               # z faces disabled in 2D
+
+
+def test_history_file_naming_and_payload(tmp_path):
+    from datetime import datetime
+
+    from deepgpr_b200.history_io import load_forward_wavefield, normalize_forward_wavefield_directory, \
+        save_forward_wavefield
+
+    d = normalize_forward_wavefield_directory(tmp_path / "hist")
+    t = datetime(2026, 1, 2, 13, 7)
+    x = torch.arange(24, dtype=torch.float32).reshape(2, 3, 4)
+    p0 = save_forward_wavefield(x, d, t)
+    p1 = save_forward_wavefield(x, d, t, metadata={"history_region": "physical", "history_origin": (1, 2, 0)})
+    assert p0.name == "forward_wavefield_13-07.pt" and p1.name == "forward_wavefield_13-07_01.pt"
+    assert torch.equal(torch.load(p0), x)
+    meta = torch.load(p1)
+    assert torch.equal(meta["wavefield"], x) and meta["history_origin"] == (1, 2, 0)
+    assert torch.equal(load_forward_wavefield(p1), x)
+    (tmp_path / "file").write_text("x")
+    with pytest.raises(NotADirectoryError):
+        normalize_forward_wavefield_directory(tmp_path / "file")
