@@ -76,6 +76,15 @@ def test_3d_two_equal_spacings(spacing, cuda_device, oracle_lib):
     _compare(got, ref, grads=("grad_eps", "grad_sigma", "grad_source"))
 
 
+@pytest.mark.parametrize("nshot", [3, 4])
+def test_3d_shot_counts(nshot, cuda_device, oracle_lib):
+    """Shots are processed in pairs by the 3D H kernel: an odd count leaves a lone last shot."""
+    p = problem_3d(nt=30, order=4, pml=3, nshot=nshot, want_source=True)
+    ref = driver.run(p, "oracle")
+    got = run_product(p, cuda_device)
+    _compare(got, ref, grads=("grad_eps", "grad_sigma", "grad_source"))
+
+
 def test_3d_anisotropic_spacing_and_mu(cuda_device, oracle_lib):
     p = problem_3d(nt=30, order=4, pml=3, dx=(0.02, 0.017, 0.013), dt=1.0e-11)
     p.mu_r = 1.0 + 0.1 * torch.rand(p.eps_r.shape, generator=torch.Generator().manual_seed(3))
