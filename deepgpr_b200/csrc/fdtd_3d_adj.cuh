@@ -224,7 +224,7 @@ __host__ __device__ constexpr int k3_adj_smem_bytes() {
 // then the H-CPML weights of step it at the cell (deepgpr_cpu.c:1331-1396).
 // ---------------------------------------------------------------------------
 template <typename T, int R, bool EQ, bool GEN>
-__global__ void __launch_bounds__(32 * K3_WARPS, k3_min_blocks<T, R>())
+__global__ void __launch_bounds__(32 * K3_WARPS, k3_adj_min_blocks<T, R>())
     k3v_adj_e(const __grid_constant__ TiledAdj<T> P, K3Buf<T> f, K3Geom kg) {
   constexpr int ZLO = -(R - 1), ZHI = R + 1, NZN = ZHI - ZLO + 1;   // z sources of the pair, gather_back
   const AdjArgs<T>& a = P.a;
@@ -684,7 +684,7 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_min_blocks<T, R>())
 // then the head of step it-1 at the cell.
 // ---------------------------------------------------------------------------
 template <typename T, int R, bool EQ, bool GEN>
-__global__ void __launch_bounds__(32 * K3_WARPS, k3_min_blocks<T, R>())
+__global__ void __launch_bounds__(32 * K3_WARPS, k3_adj_min_blocks<T, R>())
     k3v_adj_h(const __grid_constant__ TiledAdj<T> P, K3Buf<T> f, K3Geom kg) {
   constexpr int ZLO = -R, ZHI = R, NZN = ZHI - ZLO + 1;   // z sources of the pair, gather_fwd
   const AdjArgs<T>& a = P.a;
