@@ -779,8 +779,6 @@ HBox make_box(const Grid& g, bool physical, const int* p) {
   return b;
 }
 
-long long ntiles_of(const Grid& g) { return ((long long)g.cells + kBlock - 1) / kBlock; }
-
 // FP8 scale tiles: one per (x plane, y row, 32 z columns) in 3D, one per
 // (row, 32-column strip) in 2D TM.
 long long fp8_tiles(const Grid& g, bool tm2d) {
