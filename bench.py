@@ -167,6 +167,12 @@ BYTES_PER_CELL_2D = {
     "image": 4 + 4 + 4,              # lEz, E^n, E^(n+1) per shot (per-cell terms amortised)
 }
 
+# DRAM bytes per shot-cell and launch (frame + interior kernel of a half step), measured with
+# ncu (dram__bytes_read.sum + dram__bytes_write.sum) on the config-2 grid and shot count with
+# nt = 20; the command and the per-kernel figures are in profiles/tm2d_traffic_fwi2d_config2_nt20.md.
+# Below the algorithmic bytes: the 132 MB of fields stay partly resident in the 126 MB L2.
+DRAM_BYTES_PER_CELL_2D = {"fwd_h": 18.99, "fwd_e": 14.69, "adj_e": 16.18, "adj_h": 15.05, "image": 13.41}
+
 
 def ours(args, rank, world, local):
     import deepgpr_b200 as dg
@@ -283,12 +289,7 @@ def ours(args, rank, world, local):
     shot_cells = (nx + 21) * (ny + 21) * shots   # field grid incl. halo, all shots of this rank
     alg = BYTES_PER_CELL_2D[dom] * shot_cells
     achieved = alg / (dom_ms / max(dom_n, 1) / 1e3) / 1e9
-    traffic = None
-    tf = ROOT / "profiles" / "ncu_traffic.json"
-    if tf.is_file():
-        per_cell = json.loads(tf.read_text()).get("bytes_per_shot_cell", {}).get(dom)
-        if per_cell is not None:
-            traffic = float(per_cell) * shot_cells
+    traffic = DRAM_BYTES_PER_CELL_2D[dom] * shot_cells
     total_prof = sum(v[0] for v in prof.values())
     roofline = {
         "bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
