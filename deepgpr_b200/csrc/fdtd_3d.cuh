@@ -350,13 +350,21 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_min_blocks<T, R>()) k3v_fwd_
   for (int e = 0; e < 2; ++e) zq[e] = fz == 4 ? qz0[e] : qz1[e];
   const FaceRows<T> yr = face_rows<T, false>(a.hF[2], a.hF[3], qy0 >= 0, g, 1, s, 0, qy0 >= 0 ? qy0 : qy1);
   const FaceRows<T> zr = face_rows<T, false>(a.hF[4], a.hF[5], fz == 4, g, 2, s, j, 0);
+  Prof<T> pz[2];   // CPML profile of the lane's z-face cells (fixed along x)
+#pragma unroll
+  for (int e = 0; e < 2; ++e) {
+    pz[e] = Prof<T>{T(0), T(0), T(0), T(0)};
+    if (cps && zq[e] >= 0) pz[e] = fz == 4 ? prof(a.hF[4], zq[e]) : prof(a.hF[5], zq[e]);
+  }
   __shared__ T stg[K3_WARPS][2][kStageSlots][2][32];
   T(*const sg)[kStageSlots][2][32] = stg[threadIdx.y];
   const bool onk[2] = {kl[0], kl[1]}, jl = j < NY - 1;
   // issues the CPML operands of plane i into stage b (one commit group per plane)
   auto stage = [&](int i, int b) {
-    long long bx1, bx2;
-    const int fx = cps ? xface_at<T, false>(a.hF, g, s, i, j, bx1, bx2) : -1;
+    long long bx1 = 0, bx2 = 0;
+    int fx = -1;
+    if (cps && (q_low_h(a.hF[0].p, i) >= 0 || q_high(a.hF[1].p, i, NX) >= 0))
+      fx = xface_at<T, false>(a.hF, g, s, i, j, bx1, bx2);
     if (cps && (fx >= 0 || in_y || any_zpml)) {
       const bool il = i < NX - 1;
       const T* X1 = fx == 0 ? a.hF[0].psi1 : a.hF[1].psi1;
@@ -523,12 +531,12 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_min_blocks<T, R>()) k3v_fwd_
       cp_async_wait_prev();
       const int b = (i - wp.x0) & 1;
       const bool il = i < NX - 1;
-      long long bx1, bx2;
-      const int fx = xface_at<T, false>(a.hF, g, s, i, j, bx1, bx2);
       T up[2];
 #pragma unroll
       for (int e = 0; e < 2; ++e) up[e] = (kv[e] && (in_x || in_y || zq[e] >= 0)) ? sg[b][6][e][lane] : T(0);
       if (in_x) {
+        long long bx1, bx2;
+        const int fx = xface_at<T, false>(a.hF, g, s, i, j, bx1, bx2);
         const Prof<T> pr = fx == 0 ? prof(a.hF[0], qx0) : prof(a.hF[1], qx1);
         T* X1 = fx == 0 ? a.hF[0].psi1 : a.hF[1].psi1;
         T* X2 = fx == 0 ? a.hF[0].psi2 : a.hF[1].psi2;
@@ -553,7 +561,7 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_min_blocks<T, R>()) k3v_fwd_
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
         if (zq[e] < 0) continue;
-        const Prof<T> pr = fz == 4 ? prof(a.hF[4], zq[e]) : prof(a.hF[5], zq[e]);
+        const Prof<T>& pr = pz[e];
         if (jl)
           cpml_one<T>(zr.p1, (long long)i * zr.s1 + zq[e], sg[b][4][e][lane], pr, dEy_dz[e], a.ddz, up[e], true, hx[e]);
         if (il)
@@ -710,13 +718,21 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_min_blocks<T, R>()) k3v_fwd_
   for (int e = 0; e < 2; ++e) zq[e] = fz == 4 ? qz0[e] : qz1[e];
   const FaceRows<T> yr = face_rows<T, true>(a.eF[2], a.eF[3], qy0 >= 0, g, 1, s, 0, qy0 >= 0 ? qy0 : qy1);
   const FaceRows<T> zr = face_rows<T, true>(a.eF[4], a.eF[5], fz == 4, g, 2, s, j, 0);
+  Prof<T> pz[2];   // CPML profile of the lane's z-face cells (fixed along x)
+#pragma unroll
+  for (int e = 0; e < 2; ++e) {
+    pz[e] = Prof<T>{T(0), T(0), T(0), T(0)};
+    if (cps && zq[e] >= 0) pz[e] = fz == 4 ? prof(a.eF[4], zq[e]) : prof(a.eF[5], zq[e]);
+  }
   __shared__ T stg[K3_WARPS][2][kStageSlots][2][32];
   T(*const sg)[kStageSlots][2][32] = stg[threadIdx.y];
   const bool onk[2] = {kl[0], kl[1]}, jl = j < NY - 1;
   // issues the CPML operands and the curl-rhs coefficient of plane i into stage b
   auto stage = [&](int i, int b) {
-    long long bx1, bx2;
-    const int fx = cps ? xface_at<T, true>(a.eF, g, s, i, j, bx1, bx2) : -1;
+    long long bx1 = 0, bx2 = 0;
+    int fx = -1;
+    if (cps && i > 0 && (q_low_e(a.eF[0].p, i) >= 0 || q_high(a.eF[1].p, i, NX) >= 0))
+      fx = xface_at<T, true>(a.eF, g, s, i, j, bx1, bx2);
     if (save_r || (cps && (fx >= 0 || in_y || any_zpml))) {
       const bool il = i < NX - 1;
       const T* X1 = fx == 0 ? a.eF[0].psi1 : a.eF[1].psi1;
@@ -866,9 +882,9 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_min_blocks<T, R>()) k3v_fwd_
     if (cps && (in_x || in_y || any_zpml)) {
       // staged operands of this plane; faces update in the reference order x, y, z
       const bool il = i < NX - 1;
-      long long bx1, bx2;
-      const int fx = xface_at<T, true>(a.eF, g, s, i, j, bx1, bx2);
       if (in_x) {
+        long long bx1, bx2;
+        const int fx = xface_at<T, true>(a.eF, g, s, i, j, bx1, bx2);
         const Prof<T> pr = fx == 0 ? prof(a.eF[0], qx0) : prof(a.eF[1], qx1);
         T* X1 = fx == 0 ? a.eF[0].psi1 : a.eF[1].psi1;
         T* X2 = fx == 0 ? a.eF[0].psi2 : a.eF[1].psi2;
@@ -893,7 +909,7 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_min_blocks<T, R>()) k3v_fwd_
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
         if (zq[e] < 0) continue;
-        const Prof<T> pr = fz == 4 ? prof(a.eF[4], zq[e]) : prof(a.eF[5], zq[e]);
+        const Prof<T>& pr = pz[e];
         if (il)
           cpml_one<T>(zr.p1, (long long)i * zr.s1 + zq[e], sg[b][4][e][lane], pr, dHy_dz[e], a.ddz, cb[e], false,
                       ex[e]);
