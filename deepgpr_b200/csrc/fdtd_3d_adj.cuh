@@ -193,9 +193,9 @@ __device__ __noinline__ void head_gen(const TiledAdj<T>& P, int st, int s, int i
   if (epml) e_pml_head(P.a, s, i, j, k, c, ex, ey, ez);
 }
 
-// stage slots of the adjoint kernels: 13 fixed ones, then w1, w2 of the
+// stage slots of the adjoint kernels: 11 fixed ones, then w1, w2 of the
 // y-face weights of the 2R neighbour rows of the gathers along y
-constexpr int kAdjSlots0 = 13;
+constexpr int kAdjSlots0 = 11;
 template <int R>
 __host__ __device__ constexpr int adj_slots() {
   return kAdjSlots0 + 4 * R;
@@ -205,10 +205,9 @@ enum : int {
   kStZw1 = 2, kStZw2 = 3,      // z-face weights of the lane's columns
   kStPx1 = 4, kStPx2 = 5,      // psi cotangents of the cell, x face
   kStPy1 = 6, kStPy2 = 7,      //   y face
-  kStPz1 = 8, kStPz2 = 9,      //   z face
-  kStUp = 10,                  // rhs coefficient of the cell
-  kStHw1 = 11, kStHw2 = 12,    // z-face weights of the halo column (cell 0)
-  kStY = 13                    // row m: kStY + 2 m (w1), kStY + 2 m + 1 (w2)
+  kStUp = 8,                   // rhs coefficient of the cell
+  kStHw1 = 9, kStHw2 = 10,     // z-face weights of the halo column (cell 0)
+  kStY = 11                    // row m: kStY + 2 m (w1), kStY + 2 m + 1 (w2)
 };
 // dynamic shared memory of k3v_adj_e / k3v_adj_h: two stages per warp
 template <typename T, int R>
@@ -276,8 +275,9 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_adj_min_blocks<T, R>())
   gtaps_back<T, R>(j, NY, yup, ydn);
   // CPML positions fixed for the warp / lane: E y faces of the neighbour rows
   // (bit d + R - 1), E z face of the lane's columns and of its halo column,
-  // H y face of the row, H z face of the lane's columns.  With the faces of
-  // an axis apart (cps), both columns of a lane lie in the same face or none.
+  // H y face of the row.  With the faces of an axis apart (cps), both columns
+  // of a lane lie in the same face or none, and the H z-face weights of the
+  // step are formed after this kernel by k3z_adj_hw.
   unsigned ymask = 0;
   if (pml) {
 #pragma unroll
@@ -288,17 +288,14 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_adj_min_blocks<T, R>())
       if (y >= 0 && y < NY && (q0 >= 0 || q1 >= 0)) ymask |= 1u << (d + R - 1);
     }
   }
-  int ezq[2], hzq[2], ehq = -1, qhy0 = -1, qhy1 = -1;
-  bool ezlo = false, hzlo = false;   // the lane's z faces are the low ones
+  int ezq[2], ehq = -1, qhy0 = -1, qhy1 = -1;
+  bool ezlo = false;   // the lane's z face is the low one
 #pragma unroll
   for (int e = 0; e < 2; ++e) {
     int q0, q1;
     face_q<true>(a.eF[4].p, a.eF[5].p, kk + e, NZ, q0, q1);
     ezq[e] = (cps && kv[e]) ? (q0 >= 0 ? q0 : q1) : -1;
     ezlo |= q0 >= 0;
-    face_q<false>(a.hF[4].p, a.hF[5].p, kk + e, NZ, q0, q1);
-    hzq[e] = (cps && kv[e]) ? (q0 >= 0 ? q0 : q1) : -1;
-    hzlo |= q0 >= 0;
   }
   bool ehlo = true;
   if (cps && hok) {
@@ -310,7 +307,6 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_adj_min_blocks<T, R>())
   if (cps) face_q<false>(a.hF[2].p, a.hF[3].p, j, NY, qhy0, qhy1);
   const bool hy_on = qhy0 >= 0 || qhy1 >= 0;
   const bool any_ez = __any_sync(kFullMask, ezq[0] >= 0 || ezq[1] >= 0 || ehq >= 0);
-  const bool any_hz = __any_sync(kFullMask, hzq[0] >= 0 || hzq[1] >= 0);
 
   constexpr int NSL = adj_slots<R>();
   extern __shared__ __align__(16) unsigned char k3_adj_smem[];   // k3_adj_smem_bytes<T, R>()
@@ -326,7 +322,7 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_adj_min_blocks<T, R>())
       face_q<false>(a.hF[0].p, a.hF[1].p, i, NX, qh0, qh1);
       const bool hx_on = qh0 >= 0 || qh1 >= 0;
       const bool il = i < NX - 1;
-      if (xin || hx_on || hy_on || any_ez || any_hz || ymask) {
+      if (xin || hx_on || hy_on || any_ez || ymask) {
         // E y-face weights of the neighbour rows (A_Y, C_Y sources)
 #pragma unroll
         for (int d = -(R - 1); d <= R; ++d) {
@@ -353,7 +349,7 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_adj_min_blocks<T, R>())
         const int qhx = hxlo ? qh0 : qh1, phx = hxlo ? a.hF[0].p : a.hF[1].p;
         const bool hylo = qhy0 >= 0;
         const int qhy = hylo ? qhy0 : qhy1, phy = hylo ? a.hF[2].p : a.hF[3].p;
-        const int pez = ezlo ? a.eF[4].p : a.eF[5].p, phz = hzlo ? a.hF[4].p : a.hF[5].p;
+        const int pez = ezlo ? a.eF[4].p : a.eF[5].p;
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
           const int k = kof[e];
@@ -367,8 +363,7 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_adj_min_blocks<T, R>())
               cp_async(&sg[b][kStZw2][e][lane],
                        (ezlo ? a.eF[4].w2 : a.eF[5].w2) + cpml_at32<true>(g, 2, 2, pez, s, ezq[e], i, j, k));
           }
-          const bool hz_on = hzq[e] >= 0;
-          if (kv[e] && (hx_on || hy_on || hz_on)) cp_async(&sg[b][kStUp][e][lane], f.ch_rhs + i * PS + row + e);
+          if (kv[e] && (hx_on || hy_on)) cp_async(&sg[b][kStUp][e][lane], f.ch_rhs + i * PS + row + e);
           if (hx_on) {
             T* P1 = hxlo ? a.hF[0].psi1 : a.hF[1].psi1;
             T* P2 = hxlo ? a.hF[0].psi2 : a.hF[1].psi2;
@@ -380,12 +375,6 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_adj_min_blocks<T, R>())
             T* P2 = hylo ? a.hF[2].psi2 : a.hF[3].psi2;
             if (kl[e]) cp_async(&sg[b][kStPy1][e][lane], P1 + cpml_at32<false>(g, 1, 1, phy, s, qhy, i, j, k));
             if (kv[e] && il) cp_async(&sg[b][kStPy2][e][lane], P2 + cpml_at32<false>(g, 1, 2, phy, s, qhy, i, j, k));
-          }
-          if (hz_on) {
-            T* P1 = hzlo ? a.hF[4].psi1 : a.hF[5].psi1;
-            T* P2 = hzlo ? a.hF[4].psi2 : a.hF[5].psi2;
-            if (jl) cp_async(&sg[b][kStPz1][e][lane], P1 + cpml_at32<false>(g, 2, 1, phz, s, hzq[e], i, j, k));
-            if (il) cp_async(&sg[b][kStPz2][e][lane], P2 + cpml_at32<false>(g, 2, 2, phz, s, hzq[e], i, j, k));
           }
         }
         if (ehq >= 0) {
@@ -605,16 +594,16 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_adj_min_blocks<T, R>())
       lHy[o + row] = hy[0];
       lHz[o + row] = hz[0];
     }
-    // H-CPML adjoint weights of step it at the cell
+    // H-CPML adjoint weights of step it at the cell: x and y faces here, the z
+    // faces in k3z_adj_hw
     if (cps) {
       int qh0, qh1;
       face_q<false>(a.hF[0].p, a.hF[1].p, i, NX, qh0, qh1);
       const bool hx_on = qh0 >= 0 || qh1 >= 0;
-      if (hx_on || hy_on || any_hz) {
+      if (hx_on || hy_on) {
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
-          const bool hz_on = hzq[e] >= 0;
-          if (!(kv[e] && (hx_on || hy_on || hz_on))) continue;
+          if (!kv[e]) continue;
           const T up = sg[b][kStUp][e][lane];
           const int k = kof[e];
           if (hx_on) {
@@ -643,19 +632,6 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_adj_min_blocks<T, R>())
             if (il) {
               const long long pi = cpml_at32<false>(g, 1, 2, F.p, s, q, i, j, k);
               F.w2[pi] = pml_weight_v(hz[e], a.inv_dy, up, T(1), pr, sg[b][kStPy2][e][lane], &F.psi2[pi]);
-            }
-          }
-          if (hz_on) {
-            const Face<T>& F = hzlo ? a.hF[4] : a.hF[5];
-            const int q = hzq[e];
-            const Prof<T> pr = prof(F, q);
-            if (jl) {
-              const long long pi = cpml_at32<false>(g, 2, 1, F.p, s, q, i, j, k);
-              F.w1[pi] = pml_weight_v(hx[e], a.inv_dz, up, T(1), pr, sg[b][kStPz1][e][lane], &F.psi1[pi]);
-            }
-            if (il) {
-              const long long pi = cpml_at32<false>(g, 2, 2, F.p, s, q, i, j, k);
-              F.w2[pi] = pml_weight_v(hy[e], a.inv_dz, up, T(-1), pr, sg[b][kStPz2][e][lane], &F.psi2[pi]);
             }
           }
         }
@@ -739,17 +715,15 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_adj_min_blocks<T, R>())
       if (y >= 0 && y < NY && (q0 >= 0 || q1 >= 0)) ymask |= 1u << (d + R);
     }
   }
-  int hzq[2], ezq[2], hhq = -1, qey0 = -1, qey1 = -1;
-  bool hzlo = false, ezlo = false;
+  // (E z-face weights of the next reverse step: k3z_adj_ew, after this kernel)
+  int hzq[2], hhq = -1, qey0 = -1, qey1 = -1;
+  bool hzlo = false;
 #pragma unroll
   for (int e = 0; e < 2; ++e) {
     int q0, q1;
     face_q<false>(a.hF[4].p, a.hF[5].p, kk + e, NZ, q0, q1);
     hzq[e] = (cps && kv[e]) ? (q0 >= 0 ? q0 : q1) : -1;
     hzlo |= q0 >= 0;
-    face_q<true>(a.eF[4].p, a.eF[5].p, kk + e, NZ, q0, q1);
-    ezq[e] = (cps && kv[e]) ? (q0 >= 0 ? q0 : q1) : -1;
-    ezlo |= q0 >= 0;
   }
   bool hhlo = true;
   if (cps && hok) {
@@ -761,7 +735,6 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_adj_min_blocks<T, R>())
   if (cps) face_q<true>(a.eF[2].p, a.eF[3].p, j, NY, qey0, qey1);
   const bool ey_on = qey0 >= 0 || qey1 >= 0;
   const bool any_hz = __any_sync(kFullMask, hzq[0] >= 0 || hzq[1] >= 0 || hhq >= 0);
-  const bool any_ez = __any_sync(kFullMask, ezq[0] >= 0 || ezq[1] >= 0);
   const bool heads = head >= 0;
 
   constexpr int NSL = adj_slots<R>();
@@ -777,7 +750,7 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_adj_min_blocks<T, R>())
       if (heads) face_q<true>(a.eF[0].p, a.eF[1].p, i, NX, qe0, qe1);
       const bool ex_on = qe0 >= 0 || qe1 >= 0;
       const bool il = i < NX - 1;
-      if (xin || ex_on || (heads && (ey_on || any_ez)) || any_hz || ymask) {
+      if (xin || ex_on || (heads && ey_on) || any_hz || ymask) {
         // H y-face weights of the neighbour rows (A_Y, C_Y sources)
 #pragma unroll
         for (int d = -R; d <= R - 1; ++d) {
@@ -804,7 +777,7 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_adj_min_blocks<T, R>())
         const int qex = exlo ? qe0 : qe1, pex = exlo ? a.eF[0].p : a.eF[1].p;
         const bool eylo = qey0 >= 0;
         const int qey = eylo ? qey0 : qey1, pey = eylo ? a.eF[2].p : a.eF[3].p;
-        const int phz = hzlo ? a.hF[4].p : a.hF[5].p, pez = ezlo ? a.eF[4].p : a.eF[5].p;
+        const int phz = hzlo ? a.hF[4].p : a.hF[5].p;
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
           const int k = kof[e];
@@ -819,8 +792,7 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_adj_min_blocks<T, R>())
                        (hzlo ? a.hF[4].w2 : a.hF[5].w2) + cpml_at32<false>(g, 2, 2, phz, s, hzq[e], i, j, k));
           }
           if (!heads) continue;
-          const bool ez_on = ezq[e] >= 0;
-          if (kv[e] && (ex_on || ey_on || ez_on)) cp_async(&sg[b][kStUp][e][lane], f.ce_rhs + i * PS + row + e);
+          if (kv[e] && (ex_on || ey_on)) cp_async(&sg[b][kStUp][e][lane], f.ce_rhs + i * PS + row + e);
           if (ex_on) {
             T* P1 = exlo ? a.eF[0].psi1 : a.eF[1].psi1;
             T* P2 = exlo ? a.eF[0].psi2 : a.eF[1].psi2;
@@ -832,12 +804,6 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_adj_min_blocks<T, R>())
             T* P2 = eylo ? a.eF[2].psi2 : a.eF[3].psi2;
             if (kv[e] && il) cp_async(&sg[b][kStPy1][e][lane], P1 + cpml_at32<true>(g, 1, 1, pey, s, qey, i, j, k));
             if (kl[e]) cp_async(&sg[b][kStPy2][e][lane], P2 + cpml_at32<true>(g, 1, 2, pey, s, qey, i, j, k));
-          }
-          if (ez_on) {
-            T* P1 = ezlo ? a.eF[4].psi1 : a.eF[5].psi1;
-            T* P2 = ezlo ? a.eF[4].psi2 : a.eF[5].psi2;
-            if (il) cp_async(&sg[b][kStPz1][e][lane], P1 + cpml_at32<true>(g, 2, 1, pez, s, ezq[e], i, j, k));
-            if (jl) cp_async(&sg[b][kStPz2][e][lane], P2 + cpml_at32<true>(g, 2, 2, pez, s, ezq[e], i, j, k));
           }
         }
         if (hhq >= 0) {
@@ -1055,16 +1021,16 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_adj_min_blocks<T, R>())
         for (int e = 0; e < 2; ++e)
           if (kv[e]) head_gen(P, head, s, i, j, kof[e], true, false, ex[e], ey[e], ez[e]);
       }
-      // E-CPML adjoint weights of step it-1
+      // E-CPML adjoint weights of step it-1: x and y faces here, the z faces
+      // in k3z_adj_ew
       if (cps) {
         int qe0, qe1;
         face_q<true>(a.eF[0].p, a.eF[1].p, i, NX, qe0, qe1);
         const bool ex_on = qe0 >= 0 || qe1 >= 0;
-        if (ex_on || ey_on || any_ez) {
+        if (ex_on || ey_on) {
 #pragma unroll
           for (int e = 0; e < 2; ++e) {
-            const bool ez_on = ezq[e] >= 0;
-            if (!(kv[e] && (ex_on || ey_on || ez_on))) continue;
+            if (!kv[e]) continue;
             const T up = sg[b][kStUp][e][lane];
             const int k = kof[e];
             if (ex_on) {
@@ -1093,19 +1059,6 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_adj_min_blocks<T, R>())
               if (kl[e]) {
                 const long long pi = cpml_at32<true>(g, 1, 2, F.p, s, q, i, j, k);
                 F.w2[pi] = pml_weight_v(ez[e], a.inv_dy, up, T(-1), pr, sg[b][kStPy2][e][lane], &F.psi2[pi]);
-              }
-            }
-            if (ez_on) {
-              const Face<T>& F = ezlo ? a.eF[4] : a.eF[5];
-              const int q = ezq[e];
-              const Prof<T> pr = prof(F, q);
-              if (il) {
-                const long long pi = cpml_at32<true>(g, 2, 1, F.p, s, q, i, j, k);
-                F.w1[pi] = pml_weight_v(ex[e], a.inv_dz, up, T(-1), pr, sg[b][kStPz1][e][lane], &F.psi1[pi]);
-              }
-              if (jl) {
-                const long long pi = cpml_at32<true>(g, 2, 2, F.p, s, q, i, j, k);
-                F.w2[pi] = pml_weight_v(ey[e], a.inv_dz, up, T(1), pr, sg[b][kStPz2][e][lane], &F.psi2[pi]);
               }
             }
           }
@@ -1297,6 +1250,84 @@ __global__ void __launch_bounds__(kImage3Threads) k3_image(AdjArgs<T> a, const T
     if (ACC64) a.g_sig64[gi] += acc_s64;
     else a.g_sig[gi] += acc_s;
   }
+}
+
+// ---------------------------------------------------------------------------
+// z-face CPML adjoint weights (single-face form).  Only a few lanes of a
+// z-streamed warp lie in a z face, so these per-cell weights are formed in
+// their own pass over the z-face cells once the streamed kernel of the half
+// step has stored lambda: k3z_adj_hw after k3v_adj_e (H faces of reverse step
+// it), k3z_adj_ew after k3v_adj_h (E faces of step it-1, the head of the next
+// reverse step).  A weight needs only its cell's lambda, psi cotangent and rhs
+// coefficient, and the streamed kernels neither read nor write these arrays in
+// between, so every value equals the one the streamed kernel formed before
+// (pml_weight_v, deepgpr_cpu.c:1430-1459, 1506-1534).
+// Block (32, kZfRows): x strides over the candidate z columns of a row (the
+// low face's p + 1 columns, then the high face's p + 1), y = row within the
+// block; grid (NX * ceil(NY / kZfRows), nshot).
+// ---------------------------------------------------------------------------
+constexpr int kZfRows = 8;
+
+// Calls f(i, j, k, q, low face) for every z-face cell of this thread.
+template <typename T, bool EFACE, typename Fn>
+__device__ __forceinline__ void for_zface_cells(const Face<T>* F, const Grid& g, int nyb, Fn&& fn) {
+  const int p4 = F[4].p, p5 = F[5].p, nlo = p4 + 1, nk = nlo + p5 + 1;
+  const int i = blockIdx.x / nyb;
+  const int j = (blockIdx.x - i * nyb) * kZfRows + threadIdx.y;
+  if (j >= g.NY) return;
+  for (int kc = threadIdx.x; kc < nk; kc += 32) {
+    const int k = kc < nlo ? kc : g.NZ - 1 - p5 + (kc - nlo);
+    int q0, q1;
+    face_q<EFACE>(p4, p5, k, g.NZ, q0, q1);
+    if (q0 >= 0 || q1 >= 0) fn(i, j, k, q0 >= 0 ? q0 : q1, q0 >= 0);
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(32 * kZfRows) k3z_adj_hw(const __grid_constant__ TiledAdj<T> P, K3Buf<T> f,
+                                                            K3Geom kg, int nyb) {
+  const AdjArgs<T>& a = P.a;
+  const Grid& g = a.g;
+  const int s = blockIdx.y, PS = g.NY * kg.zp;
+  for_zface_cells<T, false>(a.hF, g, nyb, [&](int i, int j, int k, int q, bool lo) {
+    const int cc = i * PS + j * kg.zp + k;
+    const long long base = (long long)s * g.NX * PS + cc;
+    const Face<T>& F = lo ? a.hF[4] : a.hF[5];
+    const Prof<T> pr = prof(F, q);
+    const T up = f.ch_rhs[cc];
+    if (j < g.NY - 1) {
+      const int pi = cpml_at32<false>(g, 2, 1, F.p, s, q, i, j, k);
+      F.w1[pi] = pml_weight_v(f.Hx[base], a.inv_dz, up, T(1), pr, F.psi1[pi], &F.psi1[pi]);
+    }
+    if (i < g.NX - 1) {
+      const int pi = cpml_at32<false>(g, 2, 2, F.p, s, q, i, j, k);
+      F.w2[pi] = pml_weight_v(f.Hy[base], a.inv_dz, up, T(-1), pr, F.psi2[pi], &F.psi2[pi]);
+    }
+  });
+}
+
+template <typename T>
+__global__ void __launch_bounds__(32 * kZfRows) k3z_adj_ew(const __grid_constant__ TiledAdj<T> P, K3Buf<T> f,
+                                                            K3Geom kg, int nyb) {
+  const AdjArgs<T>& a = P.a;
+  const Grid& g = a.g;
+  if (a.ctrl->cur - a.k_in_chunk - 1 < 0) return;   // no head after the last reverse step
+  const int s = blockIdx.y, PS = g.NY * kg.zp;
+  for_zface_cells<T, true>(a.eF, g, nyb, [&](int i, int j, int k, int q, bool lo) {
+    const int cc = i * PS + j * kg.zp + k;
+    const long long base = (long long)s * g.NX * PS + cc;
+    const Face<T>& F = lo ? a.eF[4] : a.eF[5];
+    const Prof<T> pr = prof(F, q);
+    const T up = f.ce_rhs[cc];
+    if (i < g.NX - 1) {
+      const int pi = cpml_at32<true>(g, 2, 1, F.p, s, q, i, j, k);
+      F.w1[pi] = pml_weight_v(f.Ex[base], a.inv_dz, up, T(-1), pr, F.psi1[pi], &F.psi1[pi]);
+    }
+    if (j < g.NY - 1) {
+      const int pi = cpml_at32<true>(g, 2, 2, F.p, s, q, i, j, k);
+      F.w2[pi] = pml_weight_v(f.Ey[base], a.inv_dz, up, T(1), pr, F.psi2[pi], &F.psi2[pi]);
+    }
+  });
 }
 
 }  // namespace dg

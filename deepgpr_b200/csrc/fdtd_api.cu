@@ -1423,7 +1423,8 @@ void backward_impl(const BackwardCall<T>& bc) {
     }
     const dim3 kblock(32, K3_WARPS);
     const bool eq3 = cm.dy == cm.dx && cm.dz == cm.dx;
-    const bool gen3 = has_cpml && !kg.cpml_single;
+    // general CPML form where faces of an axis may meet, or past the z-face pass's grid limit
+    const bool gen3 = has_cpml && (!kg.cpml_single || g.nshot > 65535);
     if (ok && !tm2d) {
       // the double-precision stages exceed the 48 KB default
       k3_variant<T>(R, eq3, gen3, [&](auto RR, auto E, auto G) {
@@ -1522,12 +1523,18 @@ void backward_impl(const BackwardCall<T>& bc) {
           });
         } else {
           const unsigned nb = (unsigned)kg.nblocks;
+          // single-face form: the z-face weights in their own pass after each kernel
+          const bool zpass = sizeof(T) == 4 && has_cpml && !gen3;
+          const int nyb = (g.NY + kZfRows - 1) / kZfRows;
+          const dim3 gz((unsigned)(g.NX * nyb), (unsigned)g.nshot), bz(32, kZfRows);
           timed(KK_ADJ_E, st, [&] {
             k3_variant<T>(R, eq3, gen3, [&](auto RR, auto E, auto G) {
               constexpr int r = decltype(RR)::value;
               k3v_adj_e<T, r, decltype(E)::value, decltype(G)::value>
                   <<<nb, kblock, k3_adj_smem_bytes<T, r>(), st>>>(b, kb, kg);
             });
+            if (zpass) k3z_adj_hw<T><<<gz, bz, 0, st>>>(b, kb, kg, nyb);
+            return zpass ? 2 : 1;
           });
           timed(KK_ADJ_H, st, [&] {
             k3_variant<T>(R, eq3, gen3, [&](auto RR, auto E, auto G) {
@@ -1535,6 +1542,8 @@ void backward_impl(const BackwardCall<T>& bc) {
               k3v_adj_h<T, r, decltype(E)::value, decltype(G)::value>
                   <<<nb, kblock, k3_adj_smem_bytes<T, r>(), st>>>(b, kb, kg);
             });
+            if (zpass) k3z_adj_ew<T><<<gz, bz, 0, st>>>(b, kb, kg, nyb);
+            return zpass ? 2 : 1;
           });
         }
       };
