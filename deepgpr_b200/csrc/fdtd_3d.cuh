@@ -52,6 +52,7 @@ struct K3Geom {
   const unsigned char* src_rows;   // (nshot, NX): the plane holds a source of the shot
   const unsigned char* rcv_rows;   // (nshot, NX): the plane holds a receiver of the shot
   int cpml_single;                 // along every axis the two CPML faces are >= 4 cells apart
+  int zpost_h;                     // H z-face corrections in k3z_fwd_h after k3v_fwd_h
 };
 
 // (rows, n) <-> (rows, pitch) with zero padding.
@@ -328,8 +329,8 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_min_blocks<T, R>()) k3v_fwd_
     hxz[e] = k < NZ - 1;                          // z part of upd_hx and upd_hy
     hzz[e] = NZ - 1 != 1 && k > 0 && k < NZ - 1;  // z part of upd_hz
     kl[e] = kv[e] && k < NZ - 1;
-    qz0[e] = (kv[e] && a.has_cpml) ? q_low_h(a.hF[4].p, k) : -1;
-    qz1[e] = (kv[e] && a.has_cpml) ? q_high(a.hF[5].p, k, NZ) : -1;
+    qz0[e] = (kv[e] && a.has_cpml && !kg.zpost_h) ? q_low_h(a.hF[4].p, k) : -1;
+    qz1[e] = (kv[e] && a.has_cpml && !kg.zpost_h) ? q_high(a.hF[5].p, k, NZ) : -1;
   }
   const bool zpml = qz0[0] >= 0 || qz1[0] >= 0 || qz0[1] >= 0 || qz1[1] >= 0;
   const bool any_zpml = __any_sync(kFullMask, zpml);
@@ -1042,6 +1043,62 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_min_blocks<T, R>()) k3v_fwd_
         qHy[m][e] = qHy[m + 1][e];
         qHz[m][e] = qHz[m + 1][e];
       }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// H z-face CPML corrections (single-face form) in their own pass after
+// k3v_fwd_h, which then skips them: only a few lanes of a z-streamed warp lie
+// in a z face.  The z faces are the last correction of a cell in the
+// reference order (x, y, z; deepgpr_cpu.c:980-1097) and E is not written
+// during the H half step, so correcting the stored H here with the same
+// derivative (same taps, same order) gives the same values.
+// Block (32, kZfRowsF): x strides over the candidate z columns of a row (the
+// low face's p, then the high face's p + 1), y = row within the block; grid
+// (NX * ceil(NY / kZfRowsF), nshot).
+// ---------------------------------------------------------------------------
+constexpr int kZfRowsF = 8;
+
+template <typename T, int R>
+__global__ void __launch_bounds__(32 * kZfRowsF) k3z_fwd_h(TiledFwd<T> P, K3Buf<T> f, K3Geom kg, int nyb) {
+  const FwdArgs<T>& a = P.a;
+  const Grid& g = a.g;
+  const int NX = g.NX, NY = g.NY, NZ = g.NZ;
+  const int p4 = a.hF[4].p, p5 = a.hF[5].p, nlo = p4, nk = nlo + p5 + 1;
+  const int i = blockIdx.x / nyb;
+  const int j = (blockIdx.x - i * nyb) * kZfRowsF + threadIdx.y;
+  if (j >= NY) return;
+  const int s = blockIdx.y, zp = kg.zp, PS = NY * zp;
+  const long long rbase = (long long)s * NX * PS + (long long)i * PS + j * zp;   // (s, i, j, 0)
+  const T* __restrict__ ex = f.Ex + rbase;
+  const T* __restrict__ ey = f.Ey + rbase;
+  for (int kc = threadIdx.x; kc < nk; kc += 32) {
+    const int k = kc < nlo ? kc : NZ - 1 - p5 + (kc - nlo);
+    const int q0 = q_low_h(p4, k), q1 = q_high(p5, k, NZ);
+    if (q0 < 0 && q1 < 0) continue;
+    const bool lo = q0 >= 0;
+    const int q = lo ? q0 : q1;
+    const Face<T>& F = lo ? a.hF[4] : a.hF[5];
+    const Prof<T> pr = prof(F, q);
+    T tz[R];
+    taps_fwd<T, R>(k, NZ, tz);
+    // columns outside the axis only meet zero taps
+    const auto at = [&](const T* v, int d) { return (k + d >= 0 && k + d < NZ) ? v[k + d] : T(0); };
+    const T up = f.ch_rhs[(long long)i * PS + j * zp + k];
+    if (j < NY - 1) {
+      const T d = dfwd_t<T, R>([&](int dd) { return at(ey, dd); }, tz);
+      const long long pi = psi_index(psi_dims_h(g, 2, 1, F.p), 2, s, q, i, j, 0);
+      T h = f.Hx[rbase + k];
+      cpml_one<T>(F.psi1, pi, F.psi1[pi], pr, d, a.ddz, up, true, h);
+      f.Hx[rbase + k] = h;
+    }
+    if (i < NX - 1) {
+      const T d = dfwd_t<T, R>([&](int dd) { return at(ex, dd); }, tz);
+      const long long pi = psi_index(psi_dims_h(g, 2, 2, F.p), 2, s, q, i, j, 0);
+      T h = f.Hy[rbase + k];
+      cpml_one<T>(F.psi2, pi, F.psi2[pi], pr, d, a.ddz, up, false, h);
+      f.Hy[rbase + k] = h;
+    }
   }
 }
 

@@ -1059,6 +1059,8 @@ void forward_impl(const ForwardCall<T>& fc) {
       kg.src_rows = src_rows;
       kg.rcv_rows = rcv_rows;
       kg.cpml_single = k3_cpml_single(g, cm.p);
+      // FP32 single-face form: the H z-face corrections in k3z_fwd_h
+      kg.zpost_h = sizeof(T) == 4 && a.has_cpml && kg.cpml_single && g.nshot <= 65535;
       ok = k3_alloc_pack(scratch, g, kg, cm, st, kf, fc.Ex, fc.Ey, fc.Ez, fc.Hx, fc.Hy, fc.Hz);
     }
     if (ok) {
@@ -1120,10 +1122,14 @@ void forward_impl(const ForwardCall<T>& fc) {
         } else {
           const dim3 g3((unsigned)kg.nblocks), b3(32, K3_WARPS);
           const bool gen = a.has_cpml && !kg.cpml_single;
+          const int nyb = (g.NY + kZfRowsF - 1) / kZfRowsF;
+          const dim3 gz((unsigned)(g.NX * nyb), (unsigned)g.nshot), bz(32, kZfRowsF);
           timed(KK_FWD_H, st, [&] {
             k3_variant<T>(R, eq3, gen, [&](auto RR, auto E, auto G) {
               k3v_fwd_h<T, decltype(RR)::value, decltype(E)::value, decltype(G)::value><<<g3, b3, 0, st>>>(b, kf, kg);
+              if (kg.zpost_h) k3z_fwd_h<T, decltype(RR)::value><<<gz, bz, 0, st>>>(b, kf, kg, nyb);
             });
+            return kg.zpost_h ? 2 : 1;
           });
           timed(KK_FWD_E, st, [&] {
             k3_variant<T>(R, eq3, gen, [&](auto RR, auto E, auto G) {
