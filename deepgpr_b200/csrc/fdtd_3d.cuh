@@ -53,6 +53,7 @@ struct K3Geom {
   const unsigned char* rcv_rows;   // (nshot, NX): the plane holds a receiver of the shot
   int cpml_single;                 // along every axis the two CPML faces are >= 4 cells apart
   int zpost_h;                     // H z-face corrections in k3z_fwd_h after k3v_fwd_h
+  int zpost_e;                     // E z-face cells finished in k3z_fwd_e after k3v_fwd_e (no R^n kept)
 };
 
 // (rows, n) <-> (rows, pitch) with zero padding.
@@ -678,7 +679,7 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_min_blocks<T, R>()) k3v_fwd_
   const bool hok = lane < 2 * R && hk >= 0 && hk < NZ;
   const int row = j * zp + kk;
   const int hrow = j * zp + (hok ? hk : 0);
-  bool kv[2], exz[2], ezz[2], kl[2];
+  bool kv[2], exz[2], ezz[2], kl[2], zfin[2];
   int qz0[2], qz1[2], kof[2];
 #pragma unroll
   for (int e = 0; e < 2; ++e) {
@@ -690,6 +691,9 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_min_blocks<T, R>()) k3v_fwd_
     kl[e] = kv[e] && k < NZ - 1;
     qz0[e] = (kv[e] && a.has_cpml && k > 0) ? q_low_e(a.eF[4].p, k) : -1;
     qz1[e] = (kv[e] && a.has_cpml && k > 0) ? q_high(a.eF[5].p, k, NZ) : -1;
+    // z-face cells finished by k3z_fwd_e (its correction, sources, receivers)
+    zfin[e] = kg.zpost_e && (qz0[e] >= 0 || qz1[e] >= 0);
+    if (kg.zpost_e) qz0[e] = qz1[e] = -1;
   }
   const bool zpml = qz0[0] >= 0 || qz1[0] >= 0 || qz0[1] >= 0 || qz1[1] >= 0;
   const bool any_zpml = __any_sync(kFullMask, zpml);
@@ -871,7 +875,7 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_min_blocks<T, R>()) k3v_fwd_
     for (int e = 0; e < 2; ++e) {
       zon[e] = qz0[e] >= 0 || qz1[e] >= 0;
       cell[e] = (i * NY + j) * NZ + kk + e;   // logical cell (point tables)
-      src_hit[e] = kv[e] && pts && point_hit(P.src, s, cell[e]);
+      src_hit[e] = kv[e] && !zfin[e] && pts && point_hit(P.src, s, cell[e]);
     }
     cp_async_wait_prev();
     const int b = (i - wp.x0) & 1;
@@ -1025,7 +1029,7 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_min_blocks<T, R>()) k3v_fwd_
     if (pts) {
 #pragma unroll
       for (int e = 0; e < 2; ++e)
-        if (kv[e]) sample_at(P, s, cell[e], it, ex[e], ey[e], ez[e]);
+        if (kv[e] && !zfin[e]) sample_at(P, s, cell[e], it, ex[e], ey[e], ez[e]);
     }
     if (kv[1]) {
       st2(Ex + o + row, ex);
@@ -1099,6 +1103,63 @@ __global__ void __launch_bounds__(32 * kZfRowsF) k3z_fwd_h(TiledFwd<T> P, K3Buf<
       cpml_one<T>(F.psi2, pi, F.psi2[pi], pr, d, a.ddz, up, false, h);
       f.Hy[rbase + k] = h;
     }
+  }
+}
+
+// E z-face cells (single-face form, no R^n history kept) finished in their own
+// pass after k3v_fwd_e, which stores them after the x and y faces: the z-face
+// corrections, then the cell's sources and receivers (deepgpr_cpu.c:765-880,
+// 655-666, 600-623), the reference's order.  H is not written during the E
+// half step, so the derivative (same taps, same order) is the streamed
+// kernel's.  Launch shape as k3z_fwd_h; candidate columns 1 .. p (low face),
+// then the high face's p + 1.
+template <typename T, int R>
+__global__ void __launch_bounds__(32 * kZfRowsF) k3z_fwd_e(TiledFwd<T> P, K3Buf<T> f, K3Geom kg, int nyb) {
+  const FwdArgs<T>& a = P.a;
+  const Grid& g = a.g;
+  const int NX = g.NX, NY = g.NY, NZ = g.NZ;
+  const int p4 = a.eF[4].p, p5 = a.eF[5].p, nlo = p4, nk = nlo + p5 + 1;
+  const int i = blockIdx.x / nyb;
+  const int j = (blockIdx.x - i * nyb) * kZfRowsF + threadIdx.y;
+  if (j >= NY) return;
+  const int s = blockIdx.y, zp = kg.zp, PS = NY * zp;
+  const int it = a.ctrl->cur + a.k_in_chunk;
+  const long long rbase = (long long)s * NX * PS + (long long)i * PS + j * zp;   // (s, i, j, 0)
+  const T* __restrict__ hx = f.Hx + rbase;
+  const T* __restrict__ hy = f.Hy + rbase;
+  const bool pts = (kg.src_rows && kg.src_rows[(long long)s * NX + i]) || (kg.rcv_rows && kg.rcv_rows[(long long)s * NX + i]);
+  for (int kc = threadIdx.x; kc < nk; kc += 32) {
+    const int k = kc < nlo ? kc + 1 : NZ - 1 - p5 + (kc - nlo);
+    const int q0 = q_low_e(p4, k), q1 = q_high(p5, k, NZ);
+    if (q0 < 0 && q1 < 0) continue;
+    const bool lo = q0 >= 0;
+    const int q = lo ? q0 : q1;
+    const Face<T>& F = lo ? a.eF[4] : a.eF[5];
+    const Prof<T> pr = prof(F, q);
+    T tz[R];
+    taps_back<T, R>(k, NZ, tz);
+    // columns outside the axis only meet zero taps
+    const auto at = [&](const T* v, int d) { return (k + d >= 0 && k + d < NZ) ? v[k + d] : T(0); };
+    const T cb = f.ce_rhs[(long long)i * PS + j * zp + k];
+    T ex = f.Ex[rbase + k], ey = f.Ey[rbase + k], ez = f.Ez[rbase + k];
+    if (i < NX - 1) {
+      const T d = dback_t<T, R>([&](int dd) { return at(hy, dd); }, tz);
+      const long long pi = psi_index(psi_dims_e(g, 2, 1, F.p), 2, s, q, i, j, 0);
+      cpml_one<T>(F.psi1, pi, F.psi1[pi], pr, d, a.ddz, cb, false, ex);
+    }
+    if (j < NY - 1) {
+      const T d = dback_t<T, R>([&](int dd) { return at(hx, dd); }, tz);
+      const long long pi = psi_index(psi_dims_e(g, 2, 2, F.p), 2, s, q, i, j, 0);
+      cpml_one<T>(F.psi2, pi, F.psi2[pi], pr, d, a.ddz, cb, true, ey);
+    }
+    if (pts) {
+      const int cell = (i * NY + j) * NZ + k;
+      inject_at(P, s, cell, it, cb, ex, ey, ez);
+      sample_at(P, s, cell, it, ex, ey, ez);
+    }
+    f.Ex[rbase + k] = ex;
+    f.Ey[rbase + k] = ey;
+    f.Ez[rbase + k] = ez;
   }
 }
 

@@ -1061,6 +1061,8 @@ void forward_impl(const ForwardCall<T>& fc) {
       kg.cpml_single = k3_cpml_single(g, cm.p);
       // FP32 single-face form: the H z-face corrections in k3z_fwd_h
       kg.zpost_h = sizeof(T) == 4 && a.has_cpml && kg.cpml_single && g.nshot <= 65535;
+      // and, when no R^n history is kept (its R^n needs E^n), the E z-face cells in k3z_fwd_e
+      kg.zpost_e = kg.zpost_h && !keep_r;
       ok = k3_alloc_pack(scratch, g, kg, cm, st, kf, fc.Ex, fc.Ey, fc.Ez, fc.Hx, fc.Hy, fc.Hz);
     }
     if (ok) {
@@ -1134,7 +1136,9 @@ void forward_impl(const ForwardCall<T>& fc) {
           timed(KK_FWD_E, st, [&] {
             k3_variant<T>(R, eq3, gen, [&](auto RR, auto E, auto G) {
               k3v_fwd_e<T, decltype(RR)::value, decltype(E)::value, decltype(G)::value><<<g3, b3, 0, st>>>(b, kf, kg);
+              if (kg.zpost_e) k3z_fwd_e<T, decltype(RR)::value><<<gz, bz, 0, st>>>(b, kf, kg, nyb);
             });
+            return kg.zpost_e ? 2 : 1;
           });
         }
       };
