@@ -85,6 +85,20 @@ def test_3d_shot_counts(nshot, cuda_device, oracle_lib):
     _compare(got, ref, grads=("grad_eps", "grad_sigma", "grad_source"))
 
 
+@pytest.mark.parametrize("order", [2, 4])
+def test_3d_e_only_history_points_in_the_z_faces(order, cuda_device, oracle_lib):
+    """E-only history (no stored R^n): the E z-face cells are finished after the streamed E
+    kernel, their sources and receivers included.  Physical z = 0 and z = nz - 1 lie in the
+    E z faces of the extended grid."""
+    p = problem_3d(nt=30, order=order, pml=3, rhs_from_e=True, want_source=True)
+    p.source_location = torch.tensor([[[8, 7, 0]], [[5, 6, 11]]], dtype=torch.int32)
+    p.receiver_location = torch.tensor([[[10, 3, 0], [5, 7, 11], [8, 7, 0]], [[1, 2, 11], [5, 6, 5], [5, 6, 11]]],
+                                       dtype=torch.int32)
+    ref = driver.run(p, "oracle")
+    got = run_product(p, cuda_device)
+    _compare(got, ref, grads=("grad_eps", "grad_sigma", "grad_source"))
+
+
 def test_3d_anisotropic_spacing_and_mu(cuda_device, oracle_lib):
     p = problem_3d(nt=30, order=4, pml=3, dx=(0.02, 0.017, 0.013), dt=1.0e-11)
     p.mu_r = 1.0 + 0.1 * torch.rand(p.eps_r.shape, generator=torch.Generator().manual_seed(3))
