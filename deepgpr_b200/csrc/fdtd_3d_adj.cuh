@@ -19,11 +19,12 @@
 // where the source point is outside the axis or its clamped stencil does not
 // reach the target), so the same code covers the whole grid.
 //
-// CPML operands of the next plane (E-face weights of the entering x plane and
-// of the lane's z columns, psi cotangents and the rhs coefficient of the
-// cell) are staged into shared memory with cp.async while the current plane
-// is computed (the forward kernels' scheme); y-face weights of neighbour rows
-// are loaded where they are used.
+// CPML channel weights of the next plane (of the entering x plane, of the
+// lane's z columns and of the neighbour rows' y faces) are staged into shared
+// memory with cp.async while the current plane is computed (the forward
+// kernels' scheme).  With one CPML face per axis the weights of the step
+// itself (k3v_adj_e: H faces; k3v_adj_h: E faces of the next step) are formed
+// by k3p_adj_w after the kernel.
 #pragma once
 
 #include "fdtd_3d.cuh"
@@ -193,9 +194,9 @@ __device__ __noinline__ void head_gen(const TiledAdj<T>& P, int st, int s, int i
   if (epml) e_pml_head(P.a, s, i, j, k, c, ex, ey, ez);
 }
 
-// stage slots of the adjoint kernels: 11 fixed ones, then w1, w2 of the
+// stage slots of the adjoint kernels: 6 fixed ones, then w1, w2 of the
 // y-face weights of the 2R neighbour rows of the gathers along y
-constexpr int kAdjSlots0 = 11;
+constexpr int kAdjSlots0 = 6;
 template <int R>
 __host__ __device__ constexpr int adj_slots() {
   return kAdjSlots0 + 4 * R;
@@ -203,11 +204,8 @@ __host__ __device__ constexpr int adj_slots() {
 enum : int {
   kStXw1 = 0, kStXw2 = 1,      // weights of the entering x plane's channels
   kStZw1 = 2, kStZw2 = 3,      // z-face weights of the lane's columns
-  kStPx1 = 4, kStPx2 = 5,      // psi cotangents of the cell, x face
-  kStPy1 = 6, kStPy2 = 7,      //   y face
-  kStUp = 8,                   // rhs coefficient of the cell
-  kStHw1 = 9, kStHw2 = 10,     // z-face weights of the halo column (cell 0)
-  kStY = 11                    // row m: kStY + 2 m (w1), kStY + 2 m + 1 (w2)
+  kStHw1 = 4, kStHw2 = 5,      // z-face weights of the halo column (cell 0)
+  kStY = 6                     // row m: kStY + 2 m (w1), kStY + 2 m + 1 (w2)
 };
 // dynamic shared memory of k3v_adj_e / k3v_adj_h: two stages per warp
 template <typename T, int R>
@@ -275,9 +273,9 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_adj_min_blocks<T, R>())
   gtaps_back<T, R>(j, NY, yup, ydn);
   // CPML positions fixed for the warp / lane: E y faces of the neighbour rows
   // (bit d + R - 1), E z face of the lane's columns and of its halo column,
-  // H y face of the row.  With the faces of an axis apart (cps), both columns
-  // of a lane lie in the same face or none, and the H z-face weights of the
-  // step are formed after this kernel by k3z_adj_hw.
+  // With the faces of an axis apart (cps), both columns of a lane lie in the
+  // same face or none, and the H-CPML weights of the step are formed after this
+  // kernel by k3p_adj_w.
   unsigned ymask = 0;
   if (pml) {
 #pragma unroll
@@ -288,7 +286,7 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_adj_min_blocks<T, R>())
       if (y >= 0 && y < NY && (q0 >= 0 || q1 >= 0)) ymask |= 1u << (d + R - 1);
     }
   }
-  int ezq[2], ehq = -1, qhy0 = -1, qhy1 = -1;
+  int ezq[2], ehq = -1;
   bool ezlo = false;   // the lane's z face is the low one
 #pragma unroll
   for (int e = 0; e < 2; ++e) {
@@ -304,8 +302,6 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_adj_min_blocks<T, R>())
     ehq = q0 >= 0 ? q0 : q1;
     ehlo = q0 >= 0;
   }
-  if (cps) face_q<false>(a.hF[2].p, a.hF[3].p, j, NY, qhy0, qhy1);
-  const bool hy_on = qhy0 >= 0 || qhy1 >= 0;
   const bool any_ez = __any_sync(kFullMask, ezq[0] >= 0 || ezq[1] >= 0 || ehq >= 0);
 
   constexpr int NSL = adj_slots<R>();
@@ -318,11 +314,8 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_adj_min_blocks<T, R>())
       int qa, qb;
       face_q<true>(a.eF[0].p, a.eF[1].p, xi, NX, qa, qb);
       const bool xin = xi < NX && (qa >= 0 || qb >= 0);
-      int qh0, qh1;
-      face_q<false>(a.hF[0].p, a.hF[1].p, i, NX, qh0, qh1);
-      const bool hx_on = qh0 >= 0 || qh1 >= 0;
       const bool il = i < NX - 1;
-      if (xin || hx_on || hy_on || any_ez || ymask) {
+      if (xin || any_ez || ymask) {
         // E y-face weights of the neighbour rows (A_Y, C_Y sources)
 #pragma unroll
         for (int d = -(R - 1); d <= R; ++d) {
@@ -345,10 +338,6 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_adj_min_blocks<T, R>())
         const int qx = xlo ? qa : qb, px = xlo ? a.eF[0].p : a.eF[1].p;
         const T* XW1 = xlo ? a.eF[0].w1 : a.eF[1].w1;
         const T* XW2 = xlo ? a.eF[0].w2 : a.eF[1].w2;
-        const bool hxlo = qh0 >= 0;
-        const int qhx = hxlo ? qh0 : qh1, phx = hxlo ? a.hF[0].p : a.hF[1].p;
-        const bool hylo = qhy0 >= 0;
-        const int qhy = hylo ? qhy0 : qhy1, phy = hylo ? a.hF[2].p : a.hF[3].p;
         const int pez = ezlo ? a.eF[4].p : a.eF[5].p;
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
@@ -362,19 +351,6 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_adj_min_blocks<T, R>())
             if (jl)
               cp_async(&sg[b][kStZw2][e][lane],
                        (ezlo ? a.eF[4].w2 : a.eF[5].w2) + cpml_at32<true>(g, 2, 2, pez, s, ezq[e], i, j, k));
-          }
-          if (kv[e] && (hx_on || hy_on)) cp_async(&sg[b][kStUp][e][lane], f.ch_rhs + i * PS + row + e);
-          if (hx_on) {
-            T* P1 = hxlo ? a.hF[0].psi1 : a.hF[1].psi1;
-            T* P2 = hxlo ? a.hF[0].psi2 : a.hF[1].psi2;
-            if (kl[e]) cp_async(&sg[b][kStPx1][e][lane], P1 + cpml_at32<false>(g, 0, 1, phx, s, qhx, i, j, k));
-            if (kv[e] && jl) cp_async(&sg[b][kStPx2][e][lane], P2 + cpml_at32<false>(g, 0, 2, phx, s, qhx, i, j, k));
-          }
-          if (hy_on) {
-            T* P1 = hylo ? a.hF[2].psi1 : a.hF[3].psi1;
-            T* P2 = hylo ? a.hF[2].psi2 : a.hF[3].psi2;
-            if (kl[e]) cp_async(&sg[b][kStPy1][e][lane], P1 + cpml_at32<false>(g, 1, 1, phy, s, qhy, i, j, k));
-            if (kv[e] && il) cp_async(&sg[b][kStPy2][e][lane], P2 + cpml_at32<false>(g, 1, 2, phy, s, qhy, i, j, k));
           }
         }
         if (ehq >= 0) {
@@ -594,49 +570,9 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_adj_min_blocks<T, R>())
       lHy[o + row] = hy[0];
       lHz[o + row] = hz[0];
     }
-    // H-CPML adjoint weights of step it at the cell: x and y faces here, the z
-    // faces in k3z_adj_hw
-    if (cps) {
-      int qh0, qh1;
-      face_q<false>(a.hF[0].p, a.hF[1].p, i, NX, qh0, qh1);
-      const bool hx_on = qh0 >= 0 || qh1 >= 0;
-      if (hx_on || hy_on) {
-#pragma unroll
-        for (int e = 0; e < 2; ++e) {
-          if (!kv[e]) continue;
-          const T up = sg[b][kStUp][e][lane];
-          const int k = kof[e];
-          if (hx_on) {
-            const bool lo = qh0 >= 0;
-            const Face<T>& F = lo ? a.hF[0] : a.hF[1];
-            const int q = lo ? qh0 : qh1;
-            const Prof<T> pr = prof(F, q);
-            if (kl[e]) {
-              const long long pi = cpml_at32<false>(g, 0, 1, F.p, s, q, i, j, k);
-              F.w1[pi] = pml_weight_v(hy[e], a.inv_dx, up, T(1), pr, sg[b][kStPx1][e][lane], &F.psi1[pi]);
-            }
-            if (jl) {
-              const long long pi = cpml_at32<false>(g, 0, 2, F.p, s, q, i, j, k);
-              F.w2[pi] = pml_weight_v(hz[e], a.inv_dx, up, T(-1), pr, sg[b][kStPx2][e][lane], &F.psi2[pi]);
-            }
-          }
-          if (hy_on) {
-            const bool lo = qhy0 >= 0;
-            const Face<T>& F = lo ? a.hF[2] : a.hF[3];
-            const int q = lo ? qhy0 : qhy1;
-            const Prof<T> pr = prof(F, q);
-            if (kl[e]) {
-              const long long pi = cpml_at32<false>(g, 1, 1, F.p, s, q, i, j, k);
-              F.w1[pi] = pml_weight_v(hx[e], a.inv_dy, up, T(-1), pr, sg[b][kStPy1][e][lane], &F.psi1[pi]);
-            }
-            if (il) {
-              const long long pi = cpml_at32<false>(g, 1, 2, F.p, s, q, i, j, k);
-              F.w2[pi] = pml_weight_v(hz[e], a.inv_dy, up, T(1), pr, sg[b][kStPy2][e][lane], &F.psi2[pi]);
-            }
-          }
-        }
-      }
-    } else if (GEN && pml) {
+    // H-CPML adjoint weights of step it at the cell: with one face per axis
+    // (cps) in k3p_adj_w after this kernel
+    if (GEN && pml) {
       // faces of one axis meet: every face in turn, direct loads
 #pragma unroll
       for (int e = 0; e < 2; ++e)
@@ -715,8 +651,8 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_adj_min_blocks<T, R>())
       if (y >= 0 && y < NY && (q0 >= 0 || q1 >= 0)) ymask |= 1u << (d + R);
     }
   }
-  // (E z-face weights of the next reverse step: k3z_adj_ew, after this kernel)
-  int hzq[2], hhq = -1, qey0 = -1, qey1 = -1;
+  // (E-CPML weights of the next reverse step: k3p_adj_w, after this kernel)
+  int hzq[2], hhq = -1;
   bool hzlo = false;
 #pragma unroll
   for (int e = 0; e < 2; ++e) {
@@ -732,8 +668,6 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_adj_min_blocks<T, R>())
     hhq = q0 >= 0 ? q0 : q1;
     hhlo = q0 >= 0;
   }
-  if (cps) face_q<true>(a.eF[2].p, a.eF[3].p, j, NY, qey0, qey1);
-  const bool ey_on = qey0 >= 0 || qey1 >= 0;
   const bool any_hz = __any_sync(kFullMask, hzq[0] >= 0 || hzq[1] >= 0 || hhq >= 0);
   const bool heads = head >= 0;
 
@@ -746,11 +680,8 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_adj_min_blocks<T, R>())
       int qa, qb;
       face_q<false>(a.hF[0].p, a.hF[1].p, xi, NX, qa, qb);
       const bool xin = xi < NX && (qa >= 0 || qb >= 0);
-      int qe0 = -1, qe1 = -1;
-      if (heads) face_q<true>(a.eF[0].p, a.eF[1].p, i, NX, qe0, qe1);
-      const bool ex_on = qe0 >= 0 || qe1 >= 0;
       const bool il = i < NX - 1;
-      if (xin || ex_on || (heads && ey_on) || any_hz || ymask) {
+      if (xin || any_hz || ymask) {
         // H y-face weights of the neighbour rows (A_Y, C_Y sources)
 #pragma unroll
         for (int d = -R; d <= R - 1; ++d) {
@@ -773,10 +704,6 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_adj_min_blocks<T, R>())
         const int qx = xlo ? qa : qb, px = xlo ? a.hF[0].p : a.hF[1].p;
         const T* XW1 = xlo ? a.hF[0].w1 : a.hF[1].w1;
         const T* XW2 = xlo ? a.hF[0].w2 : a.hF[1].w2;
-        const bool exlo = qe0 >= 0;
-        const int qex = exlo ? qe0 : qe1, pex = exlo ? a.eF[0].p : a.eF[1].p;
-        const bool eylo = qey0 >= 0;
-        const int qey = eylo ? qey0 : qey1, pey = eylo ? a.eF[2].p : a.eF[3].p;
         const int phz = hzlo ? a.hF[4].p : a.hF[5].p;
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
@@ -792,19 +719,6 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_adj_min_blocks<T, R>())
                        (hzlo ? a.hF[4].w2 : a.hF[5].w2) + cpml_at32<false>(g, 2, 2, phz, s, hzq[e], i, j, k));
           }
           if (!heads) continue;
-          if (kv[e] && (ex_on || ey_on)) cp_async(&sg[b][kStUp][e][lane], f.ce_rhs + i * PS + row + e);
-          if (ex_on) {
-            T* P1 = exlo ? a.eF[0].psi1 : a.eF[1].psi1;
-            T* P2 = exlo ? a.eF[0].psi2 : a.eF[1].psi2;
-            if (kv[e] && jl) cp_async(&sg[b][kStPx1][e][lane], P1 + cpml_at32<true>(g, 0, 1, pex, s, qex, i, j, k));
-            if (kl[e]) cp_async(&sg[b][kStPx2][e][lane], P2 + cpml_at32<true>(g, 0, 2, pex, s, qex, i, j, k));
-          }
-          if (ey_on) {
-            T* P1 = eylo ? a.eF[2].psi1 : a.eF[3].psi1;
-            T* P2 = eylo ? a.eF[2].psi2 : a.eF[3].psi2;
-            if (kv[e] && il) cp_async(&sg[b][kStPy1][e][lane], P1 + cpml_at32<true>(g, 1, 1, pey, s, qey, i, j, k));
-            if (kl[e]) cp_async(&sg[b][kStPy2][e][lane], P2 + cpml_at32<true>(g, 1, 2, pey, s, qey, i, j, k));
-          }
         }
         if (hhq >= 0) {
           const int ph = hhlo ? a.hF[4].p : a.hF[5].p;
@@ -1021,49 +935,9 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_adj_min_blocks<T, R>())
         for (int e = 0; e < 2; ++e)
           if (kv[e]) head_gen(P, head, s, i, j, kof[e], true, false, ex[e], ey[e], ez[e]);
       }
-      // E-CPML adjoint weights of step it-1: x and y faces here, the z faces
-      // in k3z_adj_ew
-      if (cps) {
-        int qe0, qe1;
-        face_q<true>(a.eF[0].p, a.eF[1].p, i, NX, qe0, qe1);
-        const bool ex_on = qe0 >= 0 || qe1 >= 0;
-        if (ex_on || ey_on) {
-#pragma unroll
-          for (int e = 0; e < 2; ++e) {
-            if (!kv[e]) continue;
-            const T up = sg[b][kStUp][e][lane];
-            const int k = kof[e];
-            if (ex_on) {
-              const bool lo = qe0 >= 0;
-              const Face<T>& F = lo ? a.eF[0] : a.eF[1];
-              const int q = lo ? qe0 : qe1;
-              const Prof<T> pr = prof(F, q);
-              if (jl) {
-                const long long pi = cpml_at32<true>(g, 0, 1, F.p, s, q, i, j, k);
-                F.w1[pi] = pml_weight_v(ey[e], a.inv_dx, up, T(-1), pr, sg[b][kStPx1][e][lane], &F.psi1[pi]);
-              }
-              if (kl[e]) {
-                const long long pi = cpml_at32<true>(g, 0, 2, F.p, s, q, i, j, k);
-                F.w2[pi] = pml_weight_v(ez[e], a.inv_dx, up, T(1), pr, sg[b][kStPx2][e][lane], &F.psi2[pi]);
-              }
-            }
-            if (ey_on) {
-              const bool lo = qey0 >= 0;
-              const Face<T>& F = lo ? a.eF[2] : a.eF[3];
-              const int q = lo ? qey0 : qey1;
-              const Prof<T> pr = prof(F, q);
-              if (il) {
-                const long long pi = cpml_at32<true>(g, 1, 1, F.p, s, q, i, j, k);
-                F.w1[pi] = pml_weight_v(ex[e], a.inv_dy, up, T(1), pr, sg[b][kStPy1][e][lane], &F.psi1[pi]);
-              }
-              if (kl[e]) {
-                const long long pi = cpml_at32<true>(g, 1, 2, F.p, s, q, i, j, k);
-                F.w2[pi] = pml_weight_v(ez[e], a.inv_dy, up, T(-1), pr, sg[b][kStPy2][e][lane], &F.psi2[pi]);
-              }
-            }
-          }
-        }
-      } else if (GEN && pml) {
+      // E-CPML adjoint weights of step it-1: with one face per axis (cps) in
+      // k3p_adj_w after this kernel
+      if (GEN && pml) {
 #pragma unroll
         for (int e = 0; e < 2; ++e)
           if (kv[e]) head_gen(P, head, s, i, j, kof[e], false, true, ex[e], ey[e], ez[e]);
@@ -1253,81 +1127,88 @@ __global__ void __launch_bounds__(kImage3Threads) k3_image(AdjArgs<T> a, const T
 }
 
 // ---------------------------------------------------------------------------
-// z-face CPML adjoint weights (single-face form).  Only a few lanes of a
-// z-streamed warp lie in a z face, so these per-cell weights are formed in
-// their own pass over the z-face cells once the streamed kernel of the half
-// step has stored lambda: k3z_adj_hw after k3v_adj_e (H faces of reverse step
-// it), k3z_adj_ew after k3v_adj_h (E faces of step it-1, the head of the next
-// reverse step).  A weight needs only its cell's lambda, psi cotangent and rhs
-// coefficient, and the streamed kernels neither read nor write these arrays in
-// between, so every value equals the one the streamed kernel formed before
-// (pml_weight_v, deepgpr_cpu.c:1430-1459, 1506-1534).
-// Block (32, kZfRows): x strides over the candidate z columns of a row (the
-// low face's p + 1 columns, then the high face's p + 1), y = row within the
-// block; grid (NX * ceil(NY / kZfRows), nshot).
+// CPML adjoint weights (single-face form) in their own pass over the face
+// cells once the streamed kernel of the half step has stored lambda:
+// k3p_adj_w<T, false> after k3v_adj_e (H faces of reverse step it),
+// k3p_adj_w<T, true> after k3v_adj_h (E faces of step it-1, the head of the
+// next reverse step).  A weight needs only its cell's lambda, psi cotangent
+// and rhs coefficient, and the streamed kernels neither read nor write these
+// arrays in between, so every value equals the one formed inside the streamed
+// kernels before (pml_weight_v, deepgpr_cpu.c:1430-1459, 1506-1534); the faces
+// of a cell write separate arrays, so their order does not matter.  The pass
+// keeps the streamed kernels free of the staging and arithmetic, which only
+// the lanes in a face use (in an edge z strip 5 of 32).
 // ---------------------------------------------------------------------------
-constexpr int kZfRows = 8;
 
-// Calls f(i, j, k, q, low face) for every z-face cell of this thread.
-template <typename T, bool EFACE, typename Fn>
-__device__ __forceinline__ void for_zface_cells(const Face<T>* F, const Grid& g, int nyb, Fn&& fn) {
-  const int p4 = F[4].p, p5 = F[5].p, nlo = p4 + 1, nk = nlo + p5 + 1;
-  const int i = blockIdx.x / nyb;
-  const int j = (blockIdx.x - i * nyb) * kZfRows + threadIdx.y;
-  if (j >= g.NY) return;
-  for (int kc = threadIdx.x; kc < nk; kc += 32) {
-    const int k = kc < nlo ? kc : g.NZ - 1 - p5 + (kc - nlo);
-    int q0, q1;
-    face_q<EFACE>(p4, p5, k, g.NZ, q0, q1);
-    if (q0 >= 0 || q1 >= 0) fn(i, j, k, q0 >= 0 ? q0 : q1, q0 >= 0);
+// Face slabs of one field (x low, x high, y low, y high, z low, z high) with
+// the other two axes whole: origin o, extents n, cumulative cell counts over
+// one shot.
+struct K3Faces {
+  int o[6][3], n[6][3];
+  unsigned cum[6];
+};
+
+// Per (field, axis): slot 1 / slot 2 weights of cell (i, j, k) from lambda
+// components l1 / l2 with signs sg1 / sg2 where the slot's extent allows
+// (the branches of the streamed kernels' former tails).
+template <typename T, bool EF>
+__global__ void __launch_bounds__(kBlock) k3p_adj_w(const __grid_constant__ TiledAdj<T> P, K3Buf<T> f, K3Geom kg,
+                                                    K3Faces fs) {
+  const AdjArgs<T>& a = P.a;
+  const Grid& g = a.g;
+  if (EF && a.ctrl->cur - a.k_in_chunk - 1 < 0) return;   // no head after the last reverse step
+  const unsigned t = blockIdx.x * kBlock + threadIdx.x;
+  if (t >= fs.cum[5]) return;
+  int b = 0;
+#pragma unroll
+  for (int q = 0; q < 5; ++q) b += t >= fs.cum[q];
+  const unsigned loc = t - (b > 0 ? fs.cum[b - 1] : 0u);
+  const unsigned nz = (unsigned)fs.n[b][2], ny = (unsigned)fs.n[b][1];
+  const unsigned rest = loc / nz, ri = rest / ny;
+  const int k = fs.o[b][2] + int(loc - rest * nz);
+  const int j = fs.o[b][1] + int(rest - ri * ny);
+  const int i = fs.o[b][0] + int(ri);
+  const int s = blockIdx.y, axis = b >> 1;
+  const Face<T>* FF = EF ? a.eF : a.hF;
+  const int plo = axis == 0 ? FF[0].p : (axis == 1 ? FF[2].p : FF[4].p);
+  const int phi = axis == 0 ? FF[1].p : (axis == 1 ? FF[3].p : FF[5].p);
+  const int c = axis == 0 ? i : (axis == 1 ? j : k);
+  const int n = axis == 0 ? g.NX : (axis == 1 ? g.NY : g.NZ);
+  int q0, q1;
+  face_q<EF>(plo, phi, c, n, q0, q1);
+  const int q = (b & 1) ? q1 : q0;
+  const Face<T>& F = b == 0 ? FF[0] : b == 1 ? FF[1] : b == 2 ? FF[2] : b == 3 ? FF[3] : b == 4 ? FF[4] : FF[5];
+  const Prof<T> pr = prof(F, q);
+  const int PS = g.NY * kg.zp, cc = i * PS + j * kg.zp + k;
+  const long long base = (long long)s * g.NX * PS + cc;
+  const T up = EF ? f.ce_rhs[cc] : f.ch_rhs[cc];
+  const T inv = axis == 0 ? a.inv_dx : (axis == 1 ? a.inv_dy : a.inv_dz);
+  const bool il = i < g.NX - 1, jl = j < g.NY - 1, kl = k < g.NZ - 1;
+  const T* l1;
+  const T* l2;
+  bool on1, on2;
+  T sg1;
+  if (!EF) {   // H faces: x (Hy, Hz), y (Hx, Hz), z (Hx, Hy)
+    l1 = axis == 0 ? f.Hy : f.Hx;
+    l2 = axis == 2 ? f.Hy : f.Hz;
+    on1 = axis == 2 ? jl : kl;
+    on2 = axis == 0 ? jl : il;
+    sg1 = axis == 1 ? T(-1) : T(1);
+  } else {     // E faces: x (Ey, Ez), y (Ex, Ez), z (Ex, Ey)
+    l1 = axis == 0 ? f.Ey : f.Ex;
+    l2 = axis == 2 ? f.Ey : f.Ez;
+    on1 = axis == 0 ? jl : il;
+    on2 = axis == 2 ? jl : kl;
+    sg1 = axis == 1 ? T(1) : T(-1);
   }
-}
-
-template <typename T>
-__global__ void __launch_bounds__(32 * kZfRows) k3z_adj_hw(const __grid_constant__ TiledAdj<T> P, K3Buf<T> f,
-                                                            K3Geom kg, int nyb) {
-  const AdjArgs<T>& a = P.a;
-  const Grid& g = a.g;
-  const int s = blockIdx.y, PS = g.NY * kg.zp;
-  for_zface_cells<T, false>(a.hF, g, nyb, [&](int i, int j, int k, int q, bool lo) {
-    const int cc = i * PS + j * kg.zp + k;
-    const long long base = (long long)s * g.NX * PS + cc;
-    const Face<T>& F = lo ? a.hF[4] : a.hF[5];
-    const Prof<T> pr = prof(F, q);
-    const T up = f.ch_rhs[cc];
-    if (j < g.NY - 1) {
-      const int pi = cpml_at32<false>(g, 2, 1, F.p, s, q, i, j, k);
-      F.w1[pi] = pml_weight_v(f.Hx[base], a.inv_dz, up, T(1), pr, F.psi1[pi], &F.psi1[pi]);
-    }
-    if (i < g.NX - 1) {
-      const int pi = cpml_at32<false>(g, 2, 2, F.p, s, q, i, j, k);
-      F.w2[pi] = pml_weight_v(f.Hy[base], a.inv_dz, up, T(-1), pr, F.psi2[pi], &F.psi2[pi]);
-    }
-  });
-}
-
-template <typename T>
-__global__ void __launch_bounds__(32 * kZfRows) k3z_adj_ew(const __grid_constant__ TiledAdj<T> P, K3Buf<T> f,
-                                                            K3Geom kg, int nyb) {
-  const AdjArgs<T>& a = P.a;
-  const Grid& g = a.g;
-  if (a.ctrl->cur - a.k_in_chunk - 1 < 0) return;   // no head after the last reverse step
-  const int s = blockIdx.y, PS = g.NY * kg.zp;
-  for_zface_cells<T, true>(a.eF, g, nyb, [&](int i, int j, int k, int q, bool lo) {
-    const int cc = i * PS + j * kg.zp + k;
-    const long long base = (long long)s * g.NX * PS + cc;
-    const Face<T>& F = lo ? a.eF[4] : a.eF[5];
-    const Prof<T> pr = prof(F, q);
-    const T up = f.ce_rhs[cc];
-    if (i < g.NX - 1) {
-      const int pi = cpml_at32<true>(g, 2, 1, F.p, s, q, i, j, k);
-      F.w1[pi] = pml_weight_v(f.Ex[base], a.inv_dz, up, T(-1), pr, F.psi1[pi], &F.psi1[pi]);
-    }
-    if (j < g.NY - 1) {
-      const int pi = cpml_at32<true>(g, 2, 2, F.p, s, q, i, j, k);
-      F.w2[pi] = pml_weight_v(f.Ey[base], a.inv_dz, up, T(1), pr, F.psi2[pi], &F.psi2[pi]);
-    }
-  });
+  if (on1) {
+    const int pi = cpml_at32<EF>(g, axis, 1, F.p, s, q, i, j, k);
+    F.w1[pi] = pml_weight_v(l1[base], inv, up, sg1, pr, F.psi1[pi], &F.psi1[pi]);
+  }
+  if (on2) {
+    const int pi = cpml_at32<EF>(g, axis, 2, F.p, s, q, i, j, k);
+    F.w2[pi] = pml_weight_v(l2[base], inv, up, -sg1, pr, F.psi2[pi], &F.psi2[pi]);
+  }
 }
 
 }  // namespace dg

@@ -611,6 +611,28 @@ void k3_variant(int R, bool eq, bool gen, F&& f) {
 template <bool EFIELD>
 void psi_counts(const Grid& g, const int* p, long long* out);
 
+// Face slabs of k3p_adj_w for E (efield) or H: along the face axis the CPML
+// cells of the face (H: 0 .. p-1 and n-1-p .. n-2; E: 1 .. p and
+// n-1-p .. n-2), the other two axes whole.
+K3Faces k3_faces(const Grid& g, const int* p, bool efield) {
+  K3Faces fs;
+  memset(&fs, 0, sizeof(fs));
+  const int n[3] = {g.NX, g.NY, g.NZ};
+  unsigned cum = 0;
+  for (int b = 0; b < 6; ++b) {
+    const int ax = b >> 1, pf = p[b];
+    const int lo = (b & 1) ? n[ax] - 1 - pf : (efield ? 1 : 0);
+    const int cnt = pf > 0 ? pf : 0;
+    for (int d = 0; d < 3; ++d) {
+      fs.o[b][d] = d == ax ? lo : 0;
+      fs.n[b][d] = d == ax ? std::max(1, cnt) : n[d];
+    }
+    cum += (unsigned)((long long)cnt * n[(ax + 1) % 3] * n[(ax + 2) % 3]);
+    fs.cum[b] = cum;
+  }
+  return fs;
+}
+
 // The 3D kernels' single-face CPML form: along every axis the two faces are
 // at least 4 cells apart (a lane's two cells, a row and a plane lie in one
 // face at most) and every CPML array is indexed in 32 bits.
@@ -1533,17 +1555,18 @@ void backward_impl(const BackwardCall<T>& bc) {
           });
         } else {
           const unsigned nb = (unsigned)kg.nblocks;
-          // single-face form: the z-face weights in their own pass after each kernel
+          // single-face form: the CPML weights in their own pass after each kernel
           const bool zpass = sizeof(T) == 4 && has_cpml && !gen3;
-          const int nyb = (g.NY + kZfRows - 1) / kZfRows;
-          const dim3 gz((unsigned)(g.NX * nyb), (unsigned)g.nshot), bz(32, kZfRows);
+          const K3Faces fh = k3_faces(g, cm.p, false), fe = k3_faces(g, cm.p, true);
+          const dim3 gph((fh.cum[5] + kBlock - 1) / kBlock, (unsigned)g.nshot);
+          const dim3 gpe((fe.cum[5] + kBlock - 1) / kBlock, (unsigned)g.nshot);
           timed(KK_ADJ_E, st, [&] {
             k3_variant<T>(R, eq3, gen3, [&](auto RR, auto E, auto G) {
               constexpr int r = decltype(RR)::value;
               k3v_adj_e<T, r, decltype(E)::value, decltype(G)::value>
                   <<<nb, kblock, k3_adj_smem_bytes<T, r>(), st>>>(b, kb, kg);
             });
-            if (zpass) k3z_adj_hw<T><<<gz, bz, 0, st>>>(b, kb, kg, nyb);
+            if (zpass) k3p_adj_w<T, false><<<gph, kBlock, 0, st>>>(b, kb, kg, fh);
             return zpass ? 2 : 1;
           });
           timed(KK_ADJ_H, st, [&] {
@@ -1552,7 +1575,7 @@ void backward_impl(const BackwardCall<T>& bc) {
               k3v_adj_h<T, r, decltype(E)::value, decltype(G)::value>
                   <<<nb, kblock, k3_adj_smem_bytes<T, r>(), st>>>(b, kb, kg);
             });
-            if (zpass) k3z_adj_ew<T><<<gz, bz, 0, st>>>(b, kb, kg, nyb);
+            if (zpass) k3p_adj_w<T, true><<<gpe, kBlock, 0, st>>>(b, kb, kg, fe);
             return zpass ? 2 : 1;
           });
         }
