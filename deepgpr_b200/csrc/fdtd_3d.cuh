@@ -44,6 +44,23 @@ __host__ __device__ constexpr int k3_adj_min_blocks() {
   return (((R >= 4 || sizeof(T) == 8) ? 8 : 16) + K3_WARPS - 1) / K3_WARPS;
 }
 
+// CPML forms of the z-streamed forward kernels: the staged single-face form
+// (faces of an axis at least 4 cells apart), the general per-face form, and
+// none in the streamed kernel: every cell gets its base update there and the
+// CPML frame is finished by a per-cell pass kernel (k3p_fwd_e; E half step).
+constexpr int kCpmSingle = 0, kCpmGeneral = 1, kCpmPass = 2;
+
+// CPML frame of the pass form: along each axis the cells 0 .. lo-1 and
+// hi .. n-1 (each face's CPML cells plus the cell at the grid end), as six
+// disjoint boxes (x low, x high, y low and high within x's interior, z low
+// and high within x's and y's interior): origin o, extents n, cumulative cell
+// counts over one shot.
+struct K3Frame {
+  int lo[3], hi[3];
+  int o[6][3], n[6][3];
+  unsigned cum[6];
+};
+
 struct K3Geom {
   int zp;                          // z pitch of the working copy (multiple of 32)
   int nzs, nyt;                    // z strips per row, y tiles (of K3_WARPS rows) per plane
@@ -52,8 +69,8 @@ struct K3Geom {
   const unsigned char* src_rows;   // (nshot, NX): the plane holds a source of the shot
   const unsigned char* rcv_rows;   // (nshot, NX): the plane holds a receiver of the shot
   int cpml_single;                 // along every axis the two CPML faces are >= 4 cells apart
+  K3Frame fr;                      // CPML frame of the pass form (E half step)
   int zpost_h;                     // H z-face corrections in k3z_fwd_h after k3v_fwd_h
-  int zpost_e;                     // E z-face cells finished in k3z_fwd_e after k3v_fwd_e (no R^n kept)
 };
 
 // (rows, n) <-> (rows, pitch) with zero padding.
@@ -297,9 +314,10 @@ __device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wa
 constexpr int kStageSlots = 7;
 
 // ---------------------------------------------------------------------------
-// 3D H half step (+ E^n history).  EQ: dx == dy == dz (curl scale 1).
+// 3D H half step (+ E^n history).  EQ: dx == dy == dz (curl scale 1); CPM:
+// CPML form (kCpmSingle, kCpmGeneral, kCpmPass).
 // ---------------------------------------------------------------------------
-template <typename T, int R, bool EQ, bool GEN>
+template <typename T, int R, bool EQ, int CPM>
 __global__ void __launch_bounds__(32 * K3_WARPS, k3_min_blocks<T, R>()) k3v_fwd_h(TiledFwd<T> P, K3Buf<T> f, K3Geom kg) {
   constexpr int ZLO = -(R - 1), ZHI = R + 1, NZN = ZHI - ZLO + 1;   // z neighbours of the pair, dfwd
   const FwdArgs<T>& a = P.a;
@@ -316,6 +334,7 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_min_blocks<T, R>()) k3v_fwd_
   T* __restrict__ Hy = f.Hy + sbase;
   T* __restrict__ Hz = f.Hz + sbase;
   const T* __restrict__ cc = f.ch_curl;
+  const bool pml = CPM != kCpmPass && a.has_cpml;   // CPML handled in this kernel
   const int hk = k3_halo<R>(wp.k0, lane);
   const bool hok = lane < 2 * R && hk >= 0 && hk < NZ;
   const int row = j * zp + kk;                              // offset of the lane's pair in a plane
@@ -330,8 +349,8 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_min_blocks<T, R>()) k3v_fwd_
     hxz[e] = k < NZ - 1;                          // z part of upd_hx and upd_hy
     hzz[e] = NZ - 1 != 1 && k > 0 && k < NZ - 1;  // z part of upd_hz
     kl[e] = kv[e] && k < NZ - 1;
-    qz0[e] = (kv[e] && a.has_cpml && !kg.zpost_h) ? q_low_h(a.hF[4].p, k) : -1;
-    qz1[e] = (kv[e] && a.has_cpml && !kg.zpost_h) ? q_high(a.hF[5].p, k, NZ) : -1;
+    qz0[e] = (kv[e] && pml && !kg.zpost_h) ? q_low_h(a.hF[4].p, k) : -1;
+    qz1[e] = (kv[e] && pml && !kg.zpost_h) ? q_high(a.hF[5].p, k, NZ) : -1;
   }
   const bool zpml = qz0[0] >= 0 || qz1[0] >= 0 || qz0[1] >= 0 || qz1[1] >= 0;
   const bool any_zpml = __any_sync(kFullMask, zpml);
@@ -341,11 +360,11 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_min_blocks<T, R>()) k3v_fwd_
   taps_fwd<T, R>(j, NY, ty);
   // y parts (uniform over the warp)
   const bool hxy = j < NY - 1, hyy = NY - 1 != 1 && j > 0 && j < NY - 1;
-  const int qy0 = a.has_cpml ? q_low_h(a.hF[2].p, j) : -1;
-  const int qy1 = a.has_cpml ? q_high(a.hF[3].p, j, NY) : -1;
+  const int qy0 = pml ? q_low_h(a.hF[2].p, j) : -1;
+  const int qy1 = pml ? q_high(a.hF[3].p, j, NY) : -1;
   const bool in_y = qy0 >= 0 || qy1 >= 0;
   // CPML rows of the row's y face and the lane's z face (faces of one axis apart)
-  const bool cps = !GEN && a.has_cpml;   // GEN: faces of an axis may meet (general form)
+  const bool cps = CPM == kCpmSingle && pml;
   const int fz = (qz0[0] >= 0 || qz0[1] >= 0) ? 4 : 5;
   int zq[2];
 #pragma unroll
@@ -503,8 +522,8 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_min_blocks<T, R>()) k3v_fwd_
     T tx[R];
     taps_fwd<T, R>(i, NX, tx);
     const bool hxx = NX - 1 != 1 && i > 0 && i < NX - 1, hyx = i < NX - 1;
-    const int qx0 = a.has_cpml ? q_low_h(a.hF[0].p, i) : -1;
-    const int qx1 = a.has_cpml ? q_high(a.hF[1].p, i, NX) : -1;
+    const int qx0 = pml ? q_low_h(a.hF[0].p, i) : -1;
+    const int qx1 = pml ? q_high(a.hF[1].p, i, NX) : -1;
     const bool in_x = qx0 >= 0 || qx1 >= 0;
     T dEz_dy[2], dEx_dy[2], dEz_dx[2], dEy_dx[2], dEy_dz[2], dEx_dz[2], cyv[2], czv[2];
 #pragma unroll
@@ -570,7 +589,7 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_min_blocks<T, R>()) k3v_fwd_
           cpml_one<T>(zr.p2, (long long)i * zr.s2 + zq[e], sg[b][5][e][lane], pr, dEx_dz[e], a.ddz, up[e], false,
                       hy[e]);
       }
-    } else if (GEN && (in_x || in_y || any_zpml)) {
+    } else if (CPM == kCpmGeneral && (in_x || in_y || any_zpml)) {
       // faces of one axis meet: the general per-face form
       T up[2];
       bool zon[2];
@@ -657,9 +676,11 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_min_blocks<T, R>()) k3v_fwd_
 }
 
 // ---------------------------------------------------------------------------
-// 3D E half step (+ sources, R^n history, receivers).
+// 3D E half step (+ sources, R^n history, receivers).  With CPM == kCpmPass
+// the CPML frame's cells are stored after their base update; their
+// corrections, sources and receivers follow in k3p_fwd_e (no R^n kept).
 // ---------------------------------------------------------------------------
-template <typename T, int R, bool EQ, bool GEN>
+template <typename T, int R, bool EQ, int CPM>
 __global__ void __launch_bounds__(32 * K3_WARPS, k3_min_blocks<T, R>()) k3v_fwd_e(TiledFwd<T> P, K3Buf<T> f, K3Geom kg) {
   constexpr int ZLO = -R, ZHI = R, NZN = ZHI - ZLO + 1;   // z neighbours of the pair, dback
   const FwdArgs<T>& a = P.a;
@@ -675,6 +696,7 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_min_blocks<T, R>()) k3v_fwd_
   const T* __restrict__ Hx = f.Hx + sbase;
   const T* __restrict__ Hy = f.Hy + sbase;
   const T* __restrict__ Hz = f.Hz + sbase;
+  const bool pml = CPM != kCpmPass && a.has_cpml;   // CPML handled in this kernel
   const int hk = k3_halo<R>(wp.k0, lane);
   const bool hok = lane < 2 * R && hk >= 0 && hk < NZ;
   const int row = j * zp + kk;
@@ -689,11 +711,10 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_min_blocks<T, R>()) k3v_fwd_
     exz[e] = k > 0 && k < NZ - 1;   // z part of upd_ex and upd_ey
     ezz[e] = k < NZ - 1;            // z part of upd_ez
     kl[e] = kv[e] && k < NZ - 1;
-    qz0[e] = (kv[e] && a.has_cpml && k > 0) ? q_low_e(a.eF[4].p, k) : -1;
-    qz1[e] = (kv[e] && a.has_cpml && k > 0) ? q_high(a.eF[5].p, k, NZ) : -1;
-    // z-face cells finished by k3z_fwd_e (its correction, sources, receivers)
-    zfin[e] = kg.zpost_e && (qz0[e] >= 0 || qz1[e] >= 0);
-    if (kg.zpost_e) qz0[e] = qz1[e] = -1;
+    qz0[e] = (kv[e] && pml && k > 0) ? q_low_e(a.eF[4].p, k) : -1;
+    qz1[e] = (kv[e] && pml && k > 0) ? q_high(a.eF[5].p, k, NZ) : -1;
+    // cells of the CPML frame, finished by k3p_fwd_e (corrections, sources, receivers)
+    zfin[e] = CPM == kCpmPass && (k < kg.fr.lo[2] || k >= kg.fr.hi[2]);
   }
   const bool zpml = qz0[0] >= 0 || qz1[0] >= 0 || qz0[1] >= 0 || qz1[1] >= 0;
   const bool any_zpml = __any_sync(kFullMask, zpml);
@@ -702,8 +723,9 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_min_blocks<T, R>()) k3v_fwd_
   taps_back<T, R>(kk + 1, NZ, tz[1]);
   taps_back<T, R>(j, NY, ty);
   const bool exy = j > 0 && j < NY - 1, eyy = j < NY - 1;   // y parts of upd_ex / upd_ez and upd_ey
-  const int qy0 = (a.has_cpml && j > 0) ? q_low_e(a.eF[2].p, j) : -1;
-  const int qy1 = (a.has_cpml && j > 0) ? q_high(a.eF[3].p, j, NY) : -1;
+  const int qy0 = (pml && j > 0) ? q_low_e(a.eF[2].p, j) : -1;
+  const int qy1 = (pml && j > 0) ? q_high(a.eF[3].p, j, NY) : -1;
+  const bool yfin = CPM == kCpmPass && (j < kg.fr.lo[1] || j >= kg.fr.hi[1]);
   const bool in_y = qy0 >= 0 || qy1 >= 0;
   const bool degx = NY - 1 != 1 || NZ - 1 != 1, degy = NX - 1 != 1 || NZ - 1 != 1, degz = NX - 1 != 1 || NY - 1 != 1;
   const int it = a.ctrl->cur + a.k_in_chunk;
@@ -716,7 +738,7 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_min_blocks<T, R>()) k3v_fwd_
   const long long bplane = (long long)a.box.ny * a.box.nz;
   const long long h0 = (long long)(j - a.box.y0) * a.box.nz + (kk - a.box.z0);
   const long long hb = slot * a.frame + s * a.box.cells();
-  const bool cps = !GEN && a.has_cpml;   // GEN: faces of an axis may meet (general form)
+  const bool cps = CPM == kCpmSingle && pml;
   const int fz = (qz0[0] >= 0 || qz0[1] >= 0) ? 4 : 5;
   int zq[2];
 #pragma unroll
@@ -834,8 +856,9 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_min_blocks<T, R>()) k3v_fwd_
     T tx[R];
     taps_back<T, R>(i, NX, tx);
     const bool exx = i < NX - 1, eyx = i > 0 && i < NX - 1;   // x parts of upd_ex and upd_ey / upd_ez
-    const int qx0 = (a.has_cpml && i > 0) ? q_low_e(a.eF[0].p, i) : -1;
-    const int qx1 = (a.has_cpml && i > 0) ? q_high(a.eF[1].p, i, NX) : -1;
+    const int qx0 = (pml && i > 0) ? q_low_e(a.eF[0].p, i) : -1;
+    const int qx1 = (pml && i > 0) ? q_high(a.eF[1].p, i, NX) : -1;
+    const bool xfin = yfin || (CPM == kCpmPass && (i < kg.fr.lo[0] || i >= kg.fr.hi[0]));
     const bool in_x = qx0 >= 0 || qx1 >= 0;
     const bool pts = (kg.src_rows && kg.src_rows[(long long)s * NX + i]) ||
                      (kg.rcv_rows && kg.rcv_rows[(long long)s * NX + i]);
@@ -875,7 +898,7 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_min_blocks<T, R>()) k3v_fwd_
     for (int e = 0; e < 2; ++e) {
       zon[e] = qz0[e] >= 0 || qz1[e] >= 0;
       cell[e] = (i * NY + j) * NZ + kk + e;   // logical cell (point tables)
-      src_hit[e] = kv[e] && !zfin[e] && pts && point_hit(P.src, s, cell[e]);
+      src_hit[e] = kv[e] && !xfin && !zfin[e] && pts && point_hit(P.src, s, cell[e]);
     }
     cp_async_wait_prev();
     const int b = (i - wp.x0) & 1;
@@ -922,7 +945,7 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_min_blocks<T, R>()) k3v_fwd_
           cpml_one<T>(zr.p2, (long long)i * zr.s2 + zq[e], sg[b][5][e][lane], pr, dHx_dz[e], a.ddz, cb[e], true,
                       ey[e]);
       }
-    } else if (GEN && (in_x || in_y || any_zpml)) {
+    } else if (CPM == kCpmGeneral && (in_x || in_y || any_zpml)) {
       // faces of one axis meet: the general per-face form
       const bool jl = j < NY - 1, il = i < NX - 1;
       const bool onk[2] = {kl[0], kl[1]}, onj[2] = {kv[0] && jl, kv[1] && jl}, oni[2] = {kv[0] && il, kv[1] && il};
@@ -1029,7 +1052,7 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_min_blocks<T, R>()) k3v_fwd_
     if (pts) {
 #pragma unroll
       for (int e = 0; e < 2; ++e)
-        if (kv[e] && !zfin[e]) sample_at(P, s, cell[e], it, ex[e], ey[e], ez[e]);
+        if (kv[e] && !xfin && !zfin[e]) sample_at(P, s, cell[e], it, ex[e], ey[e], ez[e]);
     }
     if (kv[1]) {
       st2(Ex + o + row, ex);
@@ -1106,61 +1129,96 @@ __global__ void __launch_bounds__(32 * kZfRowsF) k3z_fwd_h(TiledFwd<T> P, K3Buf<
   }
 }
 
-// E z-face cells (single-face form, no R^n history kept) finished in their own
-// pass after k3v_fwd_e, which stores them after the x and y faces: the z-face
-// corrections, then the cell's sources and receivers (deepgpr_cpu.c:765-880,
-// 655-666, 600-623), the reference's order.  H is not written during the E
-// half step, so the derivative (same taps, same order) is the streamed
-// kernel's.  Launch shape as k3z_fwd_h; candidate columns 1 .. p (low face),
-// then the high face's p + 1.
+// ---------------------------------------------------------------------------
+// CPML frame pass of the E half step's kCpmPass form, one thread per frame
+// cell, launched on the same stream right after the streamed kernel, which
+// stored every cell's base update.  A cell's CPML corrections come after its base update
+// in the reference order (faces x0 xm y0 ym z0 zm, deepgpr_cpu.c:765-880,
+// 980-1097), and the field the derivatives read is not written during the
+// half step, so correcting the stored value here with the same derivatives
+// (d_fwd / d_back: the streamed kernels' tap tables without their zero taps)
+// gives the same values.  The pass then applies the cell's sources and
+// receivers (deepgpr_cpu.c:655-666, 600-623); it runs only when no R^n history
+// is kept (R^n needs E^n, which the streamed kernel has overwritten).  Only
+// the lanes in a face need this work (in an edge z strip 5 of 32), so the
+// streamed kernel carries none of it.  (For the H half step the same pass
+// measured slower than the streamed kernel's own x and y corrections; there
+// only the z faces move out, to k3z_fwd_h.)
+// ---------------------------------------------------------------------------
+
+// (i, j, k) of frame cell t of one shot, or false past the last one
+__device__ __forceinline__ bool k3_frame_cell(const K3Frame& fr, unsigned t, int& i, int& j, int& k) {
+  if (t >= fr.cum[5]) return false;
+  int b = 0;
+#pragma unroll
+  for (int q = 0; q < 5; ++q) b += t >= fr.cum[q];
+  const unsigned loc = t - (b > 0 ? fr.cum[b - 1] : 0u);
+  const unsigned nz = (unsigned)fr.n[b][2], ny = (unsigned)fr.n[b][1];
+  const unsigned rest = loc / nz, ri = rest / ny;
+  k = fr.o[b][2] + int(loc - rest * nz);
+  j = fr.o[b][1] + int(rest - ri * ny);
+  i = fr.o[b][0] + int(ri);
+  return true;
+}
+
 template <typename T, int R>
-__global__ void __launch_bounds__(32 * kZfRowsF) k3z_fwd_e(TiledFwd<T> P, K3Buf<T> f, K3Geom kg, int nyb) {
+__global__ void __launch_bounds__(kBlock) k3p_fwd_e(TiledFwd<T> P, K3Buf<T> f, K3Geom kg) {
   const FwdArgs<T>& a = P.a;
   const Grid& g = a.g;
-  const int NX = g.NX, NY = g.NY, NZ = g.NZ;
-  const int p4 = a.eF[4].p, p5 = a.eF[5].p, nlo = p4, nk = nlo + p5 + 1;
-  const int i = blockIdx.x / nyb;
-  const int j = (blockIdx.x - i * nyb) * kZfRowsF + threadIdx.y;
-  if (j >= NY) return;
-  const int s = blockIdx.y, zp = kg.zp, PS = NY * zp;
+  int i, j, k;
+  if (!k3_frame_cell(kg.fr, blockIdx.x * kBlock + threadIdx.x, i, j, k)) return;
+  const int s = blockIdx.y, zp = kg.zp, PS = g.NY * zp;
   const int it = a.ctrl->cur + a.k_in_chunk;
-  const long long rbase = (long long)s * NX * PS + (long long)i * PS + j * zp;   // (s, i, j, 0)
-  const T* __restrict__ hx = f.Hx + rbase;
-  const T* __restrict__ hy = f.Hy + rbase;
-  const bool pts = (kg.src_rows && kg.src_rows[(long long)s * NX + i]) || (kg.rcv_rows && kg.rcv_rows[(long long)s * NX + i]);
-  for (int kc = threadIdx.x; kc < nk; kc += 32) {
-    const int k = kc < nlo ? kc + 1 : NZ - 1 - p5 + (kc - nlo);
-    const int q0 = q_low_e(p4, k), q1 = q_high(p5, k, NZ);
-    if (q0 < 0 && q1 < 0) continue;
-    const bool lo = q0 >= 0;
-    const int q = lo ? q0 : q1;
-    const Face<T>& F = lo ? a.eF[4] : a.eF[5];
+  int qf[6];
+  qf[0] = i > 0 ? q_low_e(a.eF[0].p, i) : -1;
+  qf[1] = i > 0 ? q_high(a.eF[1].p, i, g.NX) : -1;
+  qf[2] = j > 0 ? q_low_e(a.eF[2].p, j) : -1;
+  qf[3] = j > 0 ? q_high(a.eF[3].p, j, g.NY) : -1;
+  qf[4] = k > 0 ? q_low_e(a.eF[4].p, k) : -1;
+  qf[5] = k > 0 ? q_high(a.eF[5].p, k, g.NZ) : -1;
+  const bool any_pml = qf[0] >= 0 || qf[1] >= 0 || qf[2] >= 0 || qf[3] >= 0 || qf[4] >= 0 || qf[5] >= 0;
+  const bool pts = (kg.src_rows && kg.src_rows[(long long)s * g.NX + i]) ||
+                   (kg.rcv_rows && kg.rcv_rows[(long long)s * g.NX + i]);
+  if (!(any_pml || pts)) return;
+  const int cc = i * PS + j * zp + k;
+  const long long base = (long long)s * g.NX * PS + cc;
+  const T cb = f.ce_rhs[cc];
+  const T* hx = f.Hx + base;
+  const T* hy = f.Hy + base;
+  const T* hz = f.Hz + base;
+  T ex = f.Ex[base], ey = f.Ey[base], ez = f.Ez[base];
+#pragma unroll
+  for (int fc = 0; fc < 6; ++fc) {
+    const int q = qf[fc];
+    if (q < 0) continue;
+    const Face<T>& F = a.eF[fc];
     const Prof<T> pr = prof(F, q);
-    T tz[R];
-    taps_back<T, R>(k, NZ, tz);
-    // columns outside the axis only meet zero taps
-    const auto at = [&](const T* v, int d) { return (k + d >= 0 && k + d < NZ) ? v[k + d] : T(0); };
-    const T cb = f.ce_rhs[(long long)i * PS + j * zp + k];
-    T ex = f.Ex[rbase + k], ey = f.Ey[rbase + k], ez = f.Ez[rbase + k];
-    if (i < NX - 1) {
-      const T d = dback_t<T, R>([&](int dd) { return at(hy, dd); }, tz);
-      const long long pi = psi_index(psi_dims_e(g, 2, 1, F.p), 2, s, q, i, j, 0);
-      cpml_one<T>(F.psi1, pi, F.psi1[pi], pr, d, a.ddz, cb, false, ex);
+    const int axis = fc >> 1;
+    // psi slot 1 or 2 of this face: u +-= cb (ra1 d + rb psi), d = dv / h
+    auto corr = [&](int slot, T dv, const FixedDiv<T>& hd, bool plus, T& u) {
+      T* psi = slot == 1 ? F.psi1 : F.psi2;
+      const long long pi = psi_index(psi_dims_e(g, axis, slot, F.p), axis, s, q, i, j, k);
+      cpml_one<T>(psi, pi, psi[pi], pr, dv, hd, cb, plus, u);
+    };
+    if (axis == 0) {
+      if (j < g.NY - 1) corr(1, d_back<T, R>(hz, PS, i, g.NX), a.ddx, false, ey);
+      if (k < g.NZ - 1) corr(2, d_back<T, R>(hy, PS, i, g.NX), a.ddx, true, ez);
+    } else if (axis == 1) {
+      if (i < g.NX - 1) corr(1, d_back<T, R>(hz, zp, j, g.NY), a.ddy, true, ex);
+      if (k < g.NZ - 1) corr(2, d_back<T, R>(hx, zp, j, g.NY), a.ddy, false, ez);
+    } else {
+      if (i < g.NX - 1) corr(1, d_back<T, R>(hy, 1, k, g.NZ), a.ddz, false, ex);
+      if (j < g.NY - 1) corr(2, d_back<T, R>(hx, 1, k, g.NZ), a.ddz, true, ey);
     }
-    if (j < NY - 1) {
-      const T d = dback_t<T, R>([&](int dd) { return at(hx, dd); }, tz);
-      const long long pi = psi_index(psi_dims_e(g, 2, 2, F.p), 2, s, q, i, j, 0);
-      cpml_one<T>(F.psi2, pi, F.psi2[pi], pr, d, a.ddz, cb, true, ey);
-    }
-    if (pts) {
-      const int cell = (i * NY + j) * NZ + k;
-      inject_at(P, s, cell, it, cb, ex, ey, ez);
-      sample_at(P, s, cell, it, ex, ey, ez);
-    }
-    f.Ex[rbase + k] = ex;
-    f.Ey[rbase + k] = ey;
-    f.Ez[rbase + k] = ez;
   }
+  if (pts) {
+    const int cell = (i * g.NY + j) * g.NZ + k;   // logical cell (point tables)
+    inject_at(P, s, cell, it, cb, ex, ey, ez);
+    sample_at(P, s, cell, it, ex, ey, ez);
+  }
+  f.Ex[base] = ex;
+  f.Ey[base] = ey;
+  f.Ez[base] = ez;
 }
 
 }  // namespace dg

@@ -608,6 +608,56 @@ void k3_variant(int R, bool eq, bool gen, F&& f) {
   }
 }
 
+// Calls f(R, EQ, CPM) for the forward kernels (CPM: kCpmSingle, kCpmGeneral
+// or kCpmPass).  Double precision: per-axis curl scales, general CPML form.
+template <typename T, typename F>
+void k3_fwd_variant(int R, bool eq, int cpm, F&& f) {
+  auto by_r = [&](auto E, auto C) {
+    if (R == 1) f(std::integral_constant<int, 1>(), E, C);
+    else if (R == 2) f(std::integral_constant<int, 2>(), E, C);
+    else f(std::integral_constant<int, 4>(), E, C);
+  };
+  auto by_cpm = [&](auto E) {
+    if (cpm == kCpmPass) by_r(E, std::integral_constant<int, kCpmPass>());
+    else if (cpm == kCpmGeneral) by_r(E, std::integral_constant<int, kCpmGeneral>());
+    else by_r(E, std::integral_constant<int, kCpmSingle>());
+  };
+  if constexpr (sizeof(T) == 8) {
+    by_r(std::false_type(), std::integral_constant<int, kCpmGeneral>());
+  } else {
+    if (eq) by_cpm(std::true_type());
+    else by_cpm(std::false_type());
+  }
+}
+
+// CPML frame of the forward pass form: along each axis the cells 0 .. p_lo
+// (the low face's CPML cells of E and H) and n-1-p_hi .. n-1, as six disjoint
+// boxes (x slabs whole, y slabs within x's interior, z slabs within both).
+K3Frame k3_frame(const Grid& g, const int* p) {
+  K3Frame fr;
+  memset(&fr, 0, sizeof(fr));
+  const int n[3] = {g.NX, g.NY, g.NZ};
+  for (int ax = 0; ax < 3; ++ax) {
+    fr.lo[ax] = std::min(n[ax], p[2 * ax] + 1);
+    fr.hi[ax] = std::max(fr.lo[ax], n[ax] - 1 - p[2 * ax + 1]);
+  }
+  const int x0 = fr.lo[0], x1 = fr.hi[0], y0 = fr.lo[1], y1 = fr.hi[1], z0 = fr.lo[2], z1 = fr.hi[2];
+  const int box[6][6] = {
+      {0, x0, 0, g.NY, 0, g.NZ},         {x1, g.NX - x1, 0, g.NY, 0, g.NZ},          // x low, x high
+      {x0, x1 - x0, 0, y0, 0, g.NZ},     {x0, x1 - x0, y1, g.NY - y1, 0, g.NZ},      // y low, y high
+      {x0, x1 - x0, y0, y1 - y0, 0, z0}, {x0, x1 - x0, y0, y1 - y0, z1, g.NZ - z1}};  // z low, z high
+  unsigned cum = 0;
+  for (int b = 0; b < 6; ++b) {
+    for (int ax = 0; ax < 3; ++ax) {
+      fr.o[b][ax] = box[b][2 * ax];
+      fr.n[b][ax] = std::max(1, box[b][2 * ax + 1]);   // extents of empty boxes stay divisors
+    }
+    cum += (unsigned)((long long)std::max(0, box[b][1]) * std::max(0, box[b][3]) * std::max(0, box[b][5]));
+    fr.cum[b] = cum;
+  }
+  return fr;
+}
+
 template <bool EFIELD>
 void psi_counts(const Grid& g, const int* p, long long* out);
 
@@ -653,7 +703,7 @@ K3Geom k3_layout(const Grid& g) {
   kg.nzs = (g.NZ + K3W - 1) / K3W;
   kg.nyt = (g.NY + K3_WARPS - 1) / K3_WARPS;
   int blocks = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k3v_fwd_h<float, 2, true, false>, 32 * K3_WARPS, 0) !=
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k3v_fwd_h<float, 2, true, kCpmSingle>, 32 * K3_WARPS, 0) !=
           cudaSuccess ||
       blocks < 1) {
     cudaGetLastError();
@@ -1076,15 +1126,20 @@ void forward_impl(const ForwardCall<T>& fc) {
     K3Geom kg;
     memset(&kg, 0, sizeof(kg));
     const bool eq3 = cm.dy == cm.dx && cm.dz == cm.dx;
+    // CPML form of the 3D forward kernels: in FP32 the E CPML frame is finished
+    // by the per-cell pass when no R^n history is kept (R^n needs E^n, which the
+    // streamed kernel overwrites); the H z faces by their own pass
+    const int cpm_base = (a.has_cpml && !k3_cpml_single(g, cm.p)) ? kCpmGeneral : kCpmSingle;
+    const bool pass3 = sizeof(T) == 4 && a.has_cpml && g.nshot <= 65535;
+    const int cpm_h = cpm_base;
+    const int cpm_e = (pass3 && !keep_r) ? kCpmPass : cpm_base;
     if (ok && !tm2d) {
       kg = k3_layout(g);
       kg.src_rows = src_rows;
       kg.rcv_rows = rcv_rows;
       kg.cpml_single = k3_cpml_single(g, cm.p);
-      // FP32 single-face form: the H z-face corrections in k3z_fwd_h
+      kg.fr = k3_frame(g, cm.p);
       kg.zpost_h = sizeof(T) == 4 && a.has_cpml && kg.cpml_single && g.nshot <= 65535;
-      // and, when no R^n history is kept (its R^n needs E^n), the E z-face cells in k3z_fwd_e
-      kg.zpost_e = kg.zpost_h && !keep_r;
       ok = k3_alloc_pack(scratch, g, kg, cm, st, kf, fc.Ex, fc.Ey, fc.Ez, fc.Hx, fc.Hy, fc.Hz);
     }
     if (ok) {
@@ -1145,22 +1200,22 @@ void forward_impl(const ForwardCall<T>& fc) {
           });
         } else {
           const dim3 g3((unsigned)kg.nblocks), b3(32, K3_WARPS);
-          const bool gen = a.has_cpml && !kg.cpml_single;
+          const dim3 gfr((kg.fr.cum[5] + kBlock - 1) / kBlock, (unsigned)g.nshot);
           const int nyb = (g.NY + kZfRowsF - 1) / kZfRowsF;
           const dim3 gz((unsigned)(g.NX * nyb), (unsigned)g.nshot), bz(32, kZfRowsF);
           timed(KK_FWD_H, st, [&] {
-            k3_variant<T>(R, eq3, gen, [&](auto RR, auto E, auto G) {
-              k3v_fwd_h<T, decltype(RR)::value, decltype(E)::value, decltype(G)::value><<<g3, b3, 0, st>>>(b, kf, kg);
+            k3_fwd_variant<T>(R, eq3, cpm_h, [&](auto RR, auto E, auto C) {
+              k3v_fwd_h<T, decltype(RR)::value, decltype(E)::value, decltype(C)::value><<<g3, b3, 0, st>>>(b, kf, kg);
               if (kg.zpost_h) k3z_fwd_h<T, decltype(RR)::value><<<gz, bz, 0, st>>>(b, kf, kg, nyb);
             });
             return kg.zpost_h ? 2 : 1;
           });
           timed(KK_FWD_E, st, [&] {
-            k3_variant<T>(R, eq3, gen, [&](auto RR, auto E, auto G) {
-              k3v_fwd_e<T, decltype(RR)::value, decltype(E)::value, decltype(G)::value><<<g3, b3, 0, st>>>(b, kf, kg);
-              if (kg.zpost_e) k3z_fwd_e<T, decltype(RR)::value><<<gz, bz, 0, st>>>(b, kf, kg, nyb);
+            k3_fwd_variant<T>(R, eq3, cpm_e, [&](auto RR, auto E, auto C) {
+              k3v_fwd_e<T, decltype(RR)::value, decltype(E)::value, decltype(C)::value><<<g3, b3, 0, st>>>(b, kf, kg);
+              if (cpm_e == kCpmPass) k3p_fwd_e<T, decltype(RR)::value><<<gfr, kBlock, 0, st>>>(b, kf, kg);
             });
-            return kg.zpost_e ? 2 : 1;
+            return cpm_e == kCpmPass ? 2 : 1;
           });
         }
       };
