@@ -168,9 +168,9 @@ BYTES_PER_CELL_2D = {
 }
 
 # DRAM bytes per shot-cell and launch (frame + interior kernel of a half step), measured with
-# ncu (dram__bytes_read.sum + dram__bytes_write.sum) on the config-2 grid and shot count with
-# nt = 20; the command and the per-kernel figures are in profiles/tm2d_traffic_fwi2d_config2_nt20.md.
-# Below the algorithmic bytes: the 132 MB of fields stay partly resident in the 126 MB L2.
+# ncu (dram__bytes_read.sum + dram__bytes_write.sum) on the 400 x 800 grid with 32 shots and
+# nt = 20 (one gradient evaluation).  Below the algorithmic bytes: the 132 MB of fields stay
+# partly resident in the 126 MB L2.
 DRAM_BYTES_PER_CELL_2D = {"fwd_h": 18.99, "fwd_e": 14.69, "adj_e": 16.18, "adj_h": 15.05, "image": 13.41}
 
 

@@ -20,8 +20,10 @@
 // the grid read as zero); the x and y boundary work (clamped stencils, CPML
 // faces, update predicates) is uniform over a warp and runs only on the
 // planes / rows that need it; only the first and last z strips carry per-lane
-// z boundary work.  Per-cell arithmetic is that of the reference
-// (src/DeepGPR/lib/deepgpr_cpu.c:670-1100) in the same order.
+// z boundary work.  In FP32 the H z-face CPML corrections (k3z_fwd_h) and,
+// without a stored R^n history, the E CPML frame (k3p_fwd_e) are finished by
+// per-cell passes after the streamed kernel.  Per-cell arithmetic is that of
+// the reference (src/DeepGPR/lib/deepgpr_cpu.c:670-1100) in the same order.
 #pragma once
 
 #include "fdtd_tm2d.cuh"
