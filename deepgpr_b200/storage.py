@@ -16,6 +16,7 @@ path.  FP8 histories always keep the E and R pair.
 
 from __future__ import annotations
 
+import warnings
 from typing import Any, NamedTuple, Optional, Sequence, Tuple
 
 import torch
@@ -58,6 +59,9 @@ def normalize_storage_dtype(value: Any) -> torch.dtype:
     return value
 
 
+_INT8_WARNED = False
+
+
 def normalize_compression(value: Any) -> str:
     if value is None:
         return "none"
@@ -69,9 +73,17 @@ def normalize_compression(value: Any) -> str:
     if value == "zfp":
         raise NotImplementedError("wavefield_compression='zfp' has no block decoder in this library; use 'fp8'.")
     if value == "int8":
-        raise NotImplementedError(
-            "The reference's block-INT8 history is replaced by 'fp8' (E4M3 with per-tile scales) in this library."
-        )
+        global _INT8_WARNED
+        if not _INT8_WARNED:
+            _INT8_WARNED = True
+            warnings.warn(
+                "wavefield_compression='int8' is served by this library's FP8 history (E4M3 values with one "
+                "FP32 scale per 32-value tile) instead of the reference's block-INT8 layout; gradients carry "
+                "a comparable quantisation error and saved history files hold the FP8 layout.",
+                UserWarning,
+                stacklevel=3,
+            )
+        return "fp8"
     return value
 
 

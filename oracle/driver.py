@@ -14,6 +14,7 @@ Gradients are returned on the physical model (the CPML fold applied).
 from __future__ import annotations
 
 import ctypes
+import os
 import subprocess
 import time
 from dataclasses import dataclass, field
@@ -37,7 +38,10 @@ from deepgpr_b200.storage import (
 
 HERE = Path(__file__).resolve().parent
 LIBS = {"oracle": HERE / "liboracle_fdtd.so", "ref": HERE / "_ref" / "deepgpr_cpu.so"}
-REF_SOURCE = Path("/root/reference/src/DeepGPR/lib/deepgpr_cpu.c")
+# Root of the reference checkout (read only by the build recipe and the tests
+# that pin the oracle); DEEPGPR_REFERENCE_ROOT overrides the default location.
+REFERENCE_ROOT = Path(os.environ.get("DEEPGPR_REFERENCE_ROOT", "/root/reference"))
+REF_SOURCE = REFERENCE_ROOT / "src" / "DeepGPR" / "lib" / "deepgpr_cpu.c"
 
 _loaded: Dict[str, ctypes.CDLL] = {}
 
@@ -49,7 +53,10 @@ def build(kind: str = "oracle") -> Path:
         raise FileNotFoundError("reference source tree not present and oracle/_ref not prebuilt")
     if kind == "ref" and not REF_SOURCE.is_file():
         return LIBS["ref"]
-    subprocess.run(["make", "-s", "-C", str(HERE), target], check=True)
+    cmd = ["make", "-s", "-C", str(HERE), target]
+    if kind == "ref":
+        cmd.append(f"REF_SRC_DIR={REF_SOURCE.parent}")
+    subprocess.run(cmd, check=True)
     return LIBS[kind]
 
 

@@ -52,7 +52,9 @@ def test_python_tables_match_header():
 
 
 def test_header_matches_reference_parameter_order():
-    ref = Path("/root/reference/src/DeepGPR/native/abi.py")
+    from oracle import driver
+
+    ref = driver.REFERENCE_ROOT / "src" / "DeepGPR" / "native" / "abi.py"
     if not ref.is_file():
         pytest.skip("reference tree not present")
     import types

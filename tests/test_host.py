@@ -121,10 +121,25 @@ def test_compute_option_errors_match_reference():
                    eps_r=eps, sigma=sig, mode=4)
     with pytest.raises(NotImplementedError):
         dg.compute("cuda", dx=0.02, dt=1e-11, source_amplitudes=w, source_location=src, receiver_location=rcv,
-                   eps_r=eps, sigma=sig, wavefield_compression="int8")
+                   eps_r=eps, sigma=sig, wavefield_compression="zfp")
     with pytest.raises(ValueError):
         dg.compute("cuda", dx=0.02, dt=1e-11, source_amplitudes=w, source_location=src, receiver_location=rcv,
                    eps_r=eps, sigma=sig, save_wavefield_history=False, use_async_offload=True)
+
+
+def test_int8_compression_is_served_by_fp8_with_one_warning(monkeypatch):
+    """Reference callers asking for the block-INT8 history get the FP8 history, warned once."""
+    from deepgpr_b200 import storage
+
+    monkeypatch.setattr(storage, "_INT8_WARNED", False)
+    with pytest.warns(UserWarning, match="FP8"):
+        assert storage.normalize_compression("int8") == "fp8"
+    import warnings
+
+    with warnings.catch_warnings():
+        warnings.simplefilter("error")
+        assert storage.normalize_compression("INT8") == "fp8"
+    assert storage.normalize_compression("fp8") == "fp8"
 
 
 def test_checkpoint_initial_field_shapes():
@@ -156,3 +171,35 @@ def test_history_file_naming_and_payload(tmp_path):
     (tmp_path / "file").write_text("x")
     with pytest.raises(NotADirectoryError):
         normalize_forward_wavefield_directory(tmp_path / "file")
+
+
+def test_checkpoint_plan_prefers_all_shots_then_the_longest_segments():
+    import dataclasses
+
+    from deepgpr_b200.checkpoint import history_bytes_per_step, plan_segments
+    from deepgpr_b200.solver import SolverConfig
+    from deepgpr_b200.storage import storage_config
+
+    cfg = SolverConfig(device=torch.device("cpu"), dtype=torch.float32, spacing=(0.02,) * 3, dt=1e-11, nx=100, ny=100,
+                       nz=100, nt=1000, nstep=8, nsr=1, nrx=4, pml=(10,) * 6, source_component=2,
+                       receiver_component=2, interval=1, storage=storage_config(torch.float32, "none", torch.float32),
+                       save_history=True, offload=False, fdtd_order=4, mode=3, debug=False, reconstruct_rhs=True,
+                       region="extended")
+    hist = history_bytes_per_step(cfg)
+    assert hist == 3 * 100 ** 3 * 4               # E-only mode 3, FP32, one shot
+    state = 6 * 101 ** 3 * 4
+    # everything fits: one segment, all shots
+    big = plan_segments(cfg, state, 10**13)
+    assert (big.nsegments, big.shot_batch, big.forward_passes) == (1, 8, 2)
+    # a budget of about a fifth of the history: several segments, still all shots
+    mid = plan_segments(cfg, state, 8 * hist * 200)
+    assert mid.shot_batch == 8 and 1 < mid.nsegments and mid.peak_bytes <= 8 * hist * 200
+    # too little for all shots' checkpoints: shot batches (one more forward pass)
+    small = plan_segments(cfg, state, 2 * (state * 40 + hist * 40))
+    assert small.shot_batch < 8 and small.forward_passes == 3 and small.peak_bytes <= 2 * (state * 40 + hist * 40)
+    # segments are whole multiples of the sampling interval
+    c3 = dataclasses.replace(cfg, interval=3, reconstruct_rhs=False)
+    p3 = plan_segments(c3, state, 8 * history_bytes_per_step(c3) * 100)
+    assert p3.segment_steps % 3 == 0 or p3.segment_steps == c3.nt
+    with pytest.raises(MemoryError):
+        plan_segments(cfg, state, 1000)
