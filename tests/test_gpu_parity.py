@@ -194,8 +194,10 @@ def test_fp8_history_gradient(dims, cuda_device, oracle_lib):
     ref = driver.run(p, "oracle")
     got = run_product(p, cuda_device, wavefield_compression="fp8")
     assert rel_l2(got["receivers"], ref["receivers"]) <= RX_TOL
-    assert rel_l2(got["grad_eps"], ref["grad_eps"]) < 5e-2
-    assert rel_l2(got["grad_sigma"], ref["grad_sigma"]) < 5e-2
+    # measured on B200: 2D 1.92e-2 (eps_r) / 7.7e-3 (sigma); 3D 1.25e-3 / 1.32e-3
+    eps_tol, sig_tol = (2.5e-2, 1.0e-2) if dims == 2 else (2.0e-3, 2.0e-3)
+    assert rel_l2(got["grad_eps"], ref["grad_eps"]) < eps_tol
+    assert rel_l2(got["grad_sigma"], ref["grad_sigma"]) < sig_tol
 
 
 @pytest.mark.parametrize("order", [2, 4, 8])
@@ -222,7 +224,9 @@ def test_2d_wide_grid_fp8(cuda_device, oracle_lib):
     ref = driver.run(p, "oracle")
     got = run_product(p, cuda_device, wavefield_compression="fp8")
     assert rel_l2(got["receivers"], ref["receivers"]) <= RX_TOL
-    assert rel_l2(got["grad_eps"], ref["grad_eps"]) < 5e-2
+    # measured on B200: 1.48e-2 (eps_r), 7.1e-3 (sigma)
+    assert rel_l2(got["grad_eps"], ref["grad_eps"]) < 2.0e-2
+    assert rel_l2(got["grad_sigma"], ref["grad_sigma"]) < 1.0e-2
 
 
 @pytest.mark.parametrize("divisor", [0.02, 0.015, 0.017, 0.013, 0.01, 1.0, 3.0, 0.1, 7.3e-3, 2.99e-11, 1.7e-11, 0.6931, 1e6])

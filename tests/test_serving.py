@@ -215,4 +215,5 @@ def test_fp8_served_gradient_error_against_fp64(dims, cuda_device):
     e_eps = rel_l2(got.grad_eps_r, eps.grad)
     e_sig = rel_l2(got.grad_sigma, sig.grad)
     print(f"fp8 vs fp64 ({dims}D): grad_eps {e_eps:.3e}, grad_sigma {e_sig:.3e}")
-    assert e_eps < 2e-2 and e_sig < 2e-2
+    # measured on B200: 2D 5.0e-3 / 5.4e-3, 3D 5.0e-3 / 7.0e-3 (eps_r / sigma)
+    assert e_eps < 1e-2 and e_sig < 1e-2
