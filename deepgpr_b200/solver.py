@@ -392,13 +392,14 @@ def _prepare_solve(
     if isinstance(interval, bool) or not isinstance(interval, int) or interval < 1:
         raise ValueError("model_gradient_sampling_interval must be a positive integer or 'auto'.")
     storage_dtype = normalize_storage_dtype(wavefield_storage_dtype)
+    int8_request = isinstance(wavefield_compression, str) and wavefield_compression.lower() == "int8"
     compression = normalize_compression(wavefield_compression)
     normalize_choice("wavefield_conversion_backend", wavefield_conversion_backend,
                      ("auto", "legacy", "native_scalar", "native_vec2"))
     normalize_choice("int8_reduction_backend", int8_reduction_backend, ("auto", "current", "cub_block", "warp_shuffle"))
     if wavefield_compression_rate is not None:
         raise ValueError("wavefield_compression_rate is only meaningful for the optional ZFP backend.")
-    if wavefield_compression_block_size is not None:
+    if wavefield_compression_block_size is not None and not int8_request:
         raise ValueError("wavefield_compression_block_size applies to the reference's INT8 format only.")
     if compression == "fp8" and storage_dtype != torch.float32:
         raise ValueError("wavefield_storage_dtype must stay float32 with wavefield_compression='fp8'.")
@@ -504,6 +505,8 @@ def compute(
     pml_max_velocity=SPEED_OF_LIGHT,
     precision=torch.float32,
     gradient_accumulation="float64",
+    checkpoint_segments=None,
+    checkpoint_shot_batch=None,
 ):
     """2D/3D Maxwell FDTD forward modelling with an exact discrete adjoint on B200.
 
@@ -512,11 +515,34 @@ def compute(
     ``precision``) and ``gradient_accumulation`` (``"float64"``: the material
     gradient is summed over shots and time in FP64; ``"float32"``: in FP32 in
     the reference's order).
+
+    ``checkpoint_segments`` (default ``None``: off, as the reference) runs a
+    solve whose material gradient is wanted with segment checkpointing and
+    recompute (``deepgpr_b200.checkpoint``): an integer is the segment length
+    in time steps; ``"auto"`` checkpoints only when the whole history would
+    not fit 80 % of the free device memory, with the longest segments that do.
+    ``checkpoint_shot_batch`` fixes the shots per backward batch.  A
+    checkpointed solve returns an empty ``E_saved`` (no full history exists).
     """
     args = dict(locals())
+    segments = args.pop("checkpoint_segments")
+    shot_batch = args.pop("checkpoint_shot_batch")
     output_directory = normalize_forward_wavefield_directory(save_forward_wavefield_path)
     run_time = datetime.now() if output_directory is not None else None
     cfg, tensors, prepared, states_in = _prepare_solve(**args)
+    plan = _checkpoint_plan(cfg, prepared, states_in, segments, shot_batch)
+    if plan is not None:
+        if output_directory is not None:
+            raise ValueError("save_forward_wavefield_path needs the full history; it cannot be combined with "
+                             "checkpoint_segments.")
+        if cfg.offload:
+            raise ValueError("use_async_offload=True cannot be combined with checkpoint_segments.")
+        from .checkpoint import CheckpointedFDTDFunction
+
+        outputs = CheckpointedFDTDFunction.apply(cfg, tensors, plan, prepared.eps_r, prepared.sigma,
+                                                 prepared.source_amplitudes, *states_in)
+        states, e_saved, receivers = outputs[:STATE_COUNT], outputs[STATE_COUNT], outputs[STATE_COUNT + 1]
+        return e_saved, tuple(states[0:3]), tuple(states[3:6]), tuple(states[6:30]), receivers
     outputs = FDTDFunction.apply(cfg, tensors, prepared.eps_r, prepared.sigma, prepared.source_amplitudes,
                                  *states_in)
     states, e_saved, receivers = outputs[:STATE_COUNT], outputs[STATE_COUNT], outputs[STATE_COUNT + 1]
@@ -534,6 +560,36 @@ def compute(
                             uncompressed_shape=shape)
         save_forward_wavefield(e_saved, output_directory, run_time, metadata=metadata)
     return e_saved, tuple(states[0:3]), tuple(states[3:6]), tuple(states[6:30]), receivers
+
+
+def _checkpoint_plan(cfg: SolverConfig, prepared, states, segments, shot_batch):
+    """The segment plan of a checkpointed solve, or None for a single-call solve."""
+    if segments is None or segments is False:
+        if shot_batch is not None:
+            raise ValueError("checkpoint_shot_batch needs checkpoint_segments.")
+        return None
+    auto = isinstance(segments, str)
+    if auto and segments != "auto":
+        raise ValueError("checkpoint_segments must be None, 'auto' or a positive number of time steps.")
+    if not auto and (isinstance(segments, bool) or not isinstance(segments, int) or segments < 1):
+        raise ValueError("checkpoint_segments must be None, 'auto' or a positive number of time steps.")
+    if shot_batch is not None and (isinstance(shot_batch, bool) or not isinstance(shot_batch, int)
+                                   or not 1 <= shot_batch <= cfg.nstep):
+        raise ValueError("checkpoint_shot_batch must be an integer between 1 and the shot count.")
+    if not auto and segments % cfg.interval:
+        raise ValueError("checkpoint_segments must be a multiple of model_gradient_sampling_interval.")
+    want_model = bool(prepared.eps_r.requires_grad or prepared.sigma.requires_grad)
+    if not (cfg.save_history and want_model and torch.is_grad_enabled()):
+        return None   # no history is needed: nothing to checkpoint
+    from .checkpoint import plan_segments, state_bytes_per_shot
+
+    free, _ = torch.cuda.mem_get_info(cfg.device)
+    budget = int(0.8 * free)
+    state = state_bytes_per_shot(states, cfg.nstep)
+    plan = plan_segments(cfg, state, budget, None if auto else min(segments, cfg.nt), shot_batch)
+    if auto and plan.nsegments == 1 and plan.shot_batch >= cfg.nstep:
+        return None   # the whole history fits
+    return plan
 
 
 class _DirectContext:
