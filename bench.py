@@ -72,6 +72,8 @@ def parse():
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--only-serving", action="store_true", help="print the serving object alone")
     ap.add_argument("--serving-requests", type=int, default=40)
+    ap.add_argument("--cpu-sample", action="store_true", help="time the CPU backend sample alone (internal)")
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
     return ap.parse_args()
 
 
@@ -179,12 +181,18 @@ def ours(args, rank, world, local):
     from deepgpr_b200 import native
     from deepgpr_b200.synthetic import fwi_2d
 
+    from deepgpr_b200.shots import ShotGroup, shard_acquisition
+
     dev = torch.device("cuda", local)
-    acq = fwi_2d(seed=1002 + rank, nt=args.nt, nshot=args.shots)
+    # weak scaling: the acquisition has args.shots shots per rank; each rank solves its contiguous share
+    acq = fwi_2d(seed=1002, nt=args.nt, nshot=args.shots * world)
+    acq.sources, acq.receivers, _ = shard_acquisition(acq.sources, acq.receivers, world, rank)
+    group = ShotGroup(timeout_s=120.0) if world > 1 else None
     nx, ny = acq.eps_r.shape
     ext_cells = (nx + 20) * (ny + 20)
     shots = acq.sources.shape[0]
     units_per_step = 2 * ext_cells * args.nt * shots
+    step_no = [0]
 
     common = dict(dx=acq.dx, dt=acq.dt, pmlthick=10, fdtd_order=acq.order, mode=2)
     src_d, rcv_d = acq.sources.to(dev), acq.receivers.to(dev)
@@ -204,11 +212,10 @@ def ours(args, rank, world, local):
         del out
         loss.backward()
         ge, gs = eps.grad, sig.grad
-        if world > 1:
-            import torch.distributed as dist
-
-            dist.all_reduce(ge)
-            dist.all_reduce(gs)
+        if group is not None:
+            # the one exchange of a shot-parallel gradient: sum over the ranks' shots
+            group.reduce(step_no[0], [ge, gs])
+        step_no[0] += 1
         return loss.detach(), ge, gs
 
     def barrier():
@@ -439,15 +446,33 @@ def serving_measure(dev, n=40, slots=8):
     }
 
 
-def cpu_baseline(shots: int, budget_s: float = 15.0, steps_hint: int = 0):
-    """Reference C/OpenMP backend (oracle/_ref) on a bounded sample: nt truncated."""
+def host_cpu():
+    """CPU model and the logical CPUs / physical cores this process may run on."""
+    cpus = sorted(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else list(range(os.cpu_count() or 1))
+    model, cores, cur = "unknown", set(), {}
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines() + [""]:
+            if not line.strip():
+                if cur.get("processor") is not None and int(cur["processor"]) in cpus:
+                    cores.add((cur.get("physical id", "0"), cur.get("core id", cur["processor"])))
+                    model = cur.get("model name", model)
+                cur = {}
+                continue
+            key, _, val = line.partition(":")
+            cur[key.strip()] = val.strip()
+    except OSError:
+        pass
+    return {"model": model, "logical_cpus": len(cpus), "physical_cores": len(cores) or len(cpus)}
+
+
+def cpu_sample(shots: int, budget_s: float):
+    """Reference C/OpenMP backend (oracle/_ref) on a bounded sample: nt truncated (runs in its own process)."""
     from oracle import driver
 
     from deepgpr_b200.synthetic import fwi_2d
 
     kind = "reference" if driver.available("ref") else "port"
     lib = "ref" if kind == "reference" else "oracle"
-    cores = os.cpu_count() or 1
 
     def run(nt):
         acq = fwi_2d(seed=1002, nt=nt, nshot=shots)
@@ -462,9 +487,27 @@ def cpu_baseline(shots: int, budget_s: float = 15.0, steps_hint: int = 0):
     t, acq = run(nt)
     nx, ny = acq.eps_r.shape
     units = 2 * (nx + 20) * (ny + 20) * nt * shots
-    return {"value": units / t, "unit": UNIT, "cores": cores, "kind": kind,
-            "sample": f"same workload with nt truncated to {nt} steps, {shots} shots; native forward + "
-                      f"backward time {t:.1f} s (host preprocessing excluded)"}
+    return {"value": units / t, "unit": UNIT, "kind": kind, "nt": nt, "seconds": t}
+
+
+def cpu_baseline(shots: int, budget_s: float = 15.0):
+    """The reference CPU backend timed on this host's physical cores (OMP_PROC_BIND=close), in a subprocess
+    so that the OpenMP runtime starts with that binding."""
+    info = host_cpu()
+    threads = info["physical_cores"]
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="close", OMP_PLACES="cores")
+    cmd = [sys.executable, str(Path(__file__).resolve()), "--cpu-sample", "--shots", str(shots),
+           "--cpu-budget", str(budget_s)]
+    proc = subprocess.run(cmd, env=env, capture_output=True, text=True)
+    try:
+        r = json.loads(proc.stdout.strip().splitlines()[-1])
+    except (IndexError, json.JSONDecodeError):
+        return {"error": (proc.stderr or proc.stdout)[-500:]}
+    return {"value": r["value"], "unit": UNIT, "cores": threads, "kind": r["kind"],
+            "cpu_model": info["model"], "logical_cpus": info["logical_cpus"],
+            "sample": f"same workload with nt truncated to {r['nt']} steps, {shots} shots; native forward + "
+                      f"backward time {r['seconds']:.1f} s (host preprocessing excluded); OMP_NUM_THREADS="
+                      f"{threads} (physical cores), OMP_PROC_BIND=close"}
 
 
 def reference(args, rank, world):
@@ -486,7 +529,7 @@ def reference(args, rank, world):
                    "shots": args.shots, "nt": args.nt, "fdtd_order": 4, "mode": 2,
                    "sample": "nt truncated per step (CPU)"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cpu["cores"], "kind": cpu["kind"],
-                         "sample": cpu["sample"]},
+                         "cpu_model": cpu.get("cpu_model"), "sample": cpu["sample"]},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -496,7 +539,9 @@ def main():
     args = parse()
     rank, world, local = dist_setup(args.gpus)
     try:
-        if args.impl == "reference":
+        if args.cpu_sample:
+            print(json.dumps(cpu_sample(args.shots, args.cpu_budget)), flush=True)
+        elif args.impl == "reference":
             reference(args, rank, world)
         elif args.only_serving:
             if rank == 0:
