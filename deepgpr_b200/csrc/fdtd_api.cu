@@ -15,7 +15,9 @@
 #include <algorithm>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <cmath>
 #include <atomic>
 #include <mutex>
 #include <type_traits>
@@ -24,6 +26,7 @@
 
 #include "fdtd_3d.cuh"
 #include "fdtd_3d_adj.cuh"
+#include "fdtd_3d_fast.cuh"
 
 #define DGB_API extern "C" __attribute__((visibility("default")))
 
@@ -193,27 +196,18 @@ struct Scratch {
 constexpr size_t kNoAllocScratchBytes = size_t(8) << 20;   // 8 MiB per device
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-// Address of the static scratch on the current device, looked up once per
-// device (the first dgb_forward_noalloc call on a device does this set-up).
+// Address of the static scratch on the current device.  It is looked up on
+// every call (the lookup is cheap): an address cached across calls would go
+// stale if the caller reset the device or its primary context was recreated,
+// and the module holding the array was loaded again elsewhere.
 char* noalloc_scratch_base() {
-  static std::mutex mu;
-  static char* base[64] = {};
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
-    set_error("dgb_forward_noalloc: no usable current CUDA device");
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess) {
+    set_error("dgb_forward_noalloc: cudaGetSymbolAddress of the static scratch failed: %s", cudaGetErrorString(e));
     return nullptr;
   }
-  std::lock_guard<std::mutex> lock(mu);
-  if (!base[dev]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) {
-      set_error("dgb_forward_noalloc: cudaGetSymbolAddress of the static scratch failed: %s", cudaGetErrorString(e));
-      return nullptr;
-    }
-    base[dev] = static_cast<char*>(p);
-  }
-  return base[dev];
+  return static_cast<char*>(p);
 }
 
 // Bump allocator over the static scratch, with the interface of Scratch.
@@ -937,6 +931,111 @@ bool run_loop(int steps, int dir, Control* ctrl, cudaStream_t st, Issue issue) {
   return ok;
 }
 
+// ---------------------------------------------------------------------------
+// TMA-staged 3D forward kernels (fdtd_3d_fast.cuh): launch geometry, tensor
+// maps and launches.
+// ---------------------------------------------------------------------------
+bool env_flag(const char* name) {
+  const char* v = getenv(name);
+  return v && v[0] && v[0] != '0';
+}
+
+// Whether the staged kernels take a 3D FP32 forward solve: selected with
+// DEEPGPR_B200_TMA=1, the single-face CPML form (or none), TMA plane
+// coordinates inside int32, and the driver's tensor-map encoder available.
+bool k3t_usable(const Grid& g, const int* p, bool has_cpml) {
+  if (!env_flag("DEEPGPR_B200_TMA")) return false;
+  if (has_cpml && !k3_cpml_single(g, p)) return false;
+  if ((long long)g.nshot * g.NX >= (1LL << 31)) return false;
+  return encode_tiled_fn() != nullptr;
+}
+
+template <int R>
+int k3t_resident_per_sm() {
+  return kt_min_blocks<R>();
+}
+
+// Tiles, z strips and x chunks: the chunk count keeps the last wave of CTAs
+// nearly full and each chunk long against its 2R - 1 halo planes.
+K3TGeom k3t_layout(const Grid& g, int zp, int R) {
+  K3TGeom tg;
+  memset(&tg, 0, sizeof(tg));
+  tg.zp = zp;
+  tg.nyt = (g.NY + KT_TY - 1) / KT_TY;
+  tg.nzs = (g.NZ + KT_TZ - 1) / KT_TZ;
+  const int per_sm = R >= 4 ? 1 : (R >= 2 ? 2 : 3);
+  const double resident = (double)sm_count() * per_sm;
+  const long long per = (long long)g.nshot * tg.nzs * tg.nyt;
+  int best = 1;
+  double best_eff = -1.0;
+  for (int n = 1; n <= std::max(1, std::min(64, g.NX / 8)); ++n) {
+    const int xc = (g.NX + n - 1) / n;
+    const int nch = (g.NX + xc - 1) / xc;
+    const double nb = (double)per * nch;
+    const double waves = std::ceil(nb / resident);
+    const double eff = nb / (waves * resident) * (double)xc / (xc + 2.0 * R + 2.0);
+    if (eff > best_eff + 1e-3) {
+      best_eff = eff;
+      best = n;
+    }
+  }
+  tg.xc = (g.NX + best - 1) / best;
+  tg.nchunk = (g.NX + tg.xc - 1) / tg.xc;
+  tg.nblocks = per * tg.nchunk;
+  return tg;
+}
+
+// Tensor maps of one half step (H when efield is false, E otherwise).
+template <typename T>
+bool k3t_maps(K3TMaps& m, const Grid& g, int zp, int R, const K3Buf<T>& kf, bool efield) {
+  if constexpr (sizeof(T) != 4) {
+    return false;
+  } else {
+    const long long planes = (long long)g.nshot * g.NX;
+    const T* halo[3] = {efield ? kf.Hx : kf.Ex, efield ? kf.Hy : kf.Ey, efield ? kf.Hz : kf.Ez};
+    const T* own[3] = {efield ? kf.Ex : kf.Hx, efield ? kf.Ey : kf.Hy, efield ? kf.Ez : kf.Hz};
+    const T* coef[2] = {efield ? kf.ce_hist : kf.ch_curl, efield ? kf.ce_curl : kf.ch_curl};
+    bool ok = true;
+    for (int c = 0; c < 3; ++c) {
+      ok = ok && make_map_f32(&m.halo[c], halo[c], g.NZ, zp, g.NY, planes, KT_BZ, KT_TY + 2 * R);
+      ok = ok && make_map_f32(&m.own[c], own[c], g.NZ, zp, g.NY, planes, KT_TZ, KT_TY);
+    }
+    for (int c = 0; c < 2; ++c) ok = ok && make_map_f32(&m.coef[c], coef[c], g.NZ, zp, g.NY, g.NX, KT_TZ, KT_TY);
+    if (!ok) set_error("forward: tensor map encoding failed");
+    return ok;
+  }
+}
+
+template <int R, bool EQ, bool EFIELD>
+void k3t_launch_one(unsigned nblocks, cudaStream_t st, const K3TMaps& m, const TiledFwd<float>& P,
+                    const K3Buf<float>& kf, const K3TGeom& tg) {
+  constexpr int NOWN = EFIELD ? 5 : 4;
+  constexpr size_t bytes = KtShape<R, NOWN>::BYTES;
+  auto kernel = EFIELD ? k3t_fwd_e<R, EQ> : k3t_fwd_h<R, EQ>;
+  static bool attr = [&] {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    return true;
+  }();
+  (void)attr;
+  kernel<<<nblocks, KT_THREADS, bytes, st>>>(m, P, kf, tg);
+}
+
+template <bool EFIELD>
+void k3t_launch(int R, bool eq, cudaStream_t st, const K3TMaps& m, const TiledFwd<float>& P, const K3Buf<float>& kf,
+                const K3TGeom& tg) {
+  const unsigned nb = (unsigned)tg.nblocks;
+  if (R == 1) {
+    if (eq) k3t_launch_one<1, true, EFIELD>(nb, st, m, P, kf, tg);
+    else k3t_launch_one<1, false, EFIELD>(nb, st, m, P, kf, tg);
+  } else if (R == 2) {
+    if (eq) k3t_launch_one<2, true, EFIELD>(nb, st, m, P, kf, tg);
+    else k3t_launch_one<2, false, EFIELD>(nb, st, m, P, kf, tg);
+  } else {
+    if (eq) k3t_launch_one<4, true, EFIELD>(nb, st, m, P, kf, tg);
+    else k3t_launch_one<4, false, EFIELD>(nb, st, m, P, kf, tg);
+  }
+}
+
 template <typename T>
 struct ForwardCall {
   Common<T> cm;
@@ -1142,6 +1241,18 @@ void forward_impl(const ForwardCall<T>& fc) {
       kg.zpost_h = sizeof(T) == 4 && a.has_cpml && kg.cpml_single && g.nshot <= 65535;
       ok = k3_alloc_pack(scratch, g, kg, cm, st, kf, fc.Ex, fc.Ey, fc.Ez, fc.Hx, fc.Hy, fc.Hz);
     }
+    // TMA-staged kernels for the FP32 3D forward (the z-streamed kernels otherwise)
+    const bool fast3 = sizeof(T) == 4 && ok && !tm2d && k3t_usable(g, cm.p, a.has_cpml != 0);
+    K3TGeom ktg;
+    memset(&ktg, 0, sizeof(ktg));
+    K3TMaps kmH, kmE;
+    if (fast3) {
+      ktg = k3t_layout(g, kg.zp, R);
+      ktg.src_rows = src_rows;
+      ktg.rcv_rows = rcv_rows;
+      ktg.ctrl = ctrl;
+      ok = k3t_maps(kmH, g, kg.zp, R, kf, false) && k3t_maps(kmE, g, kg.zp, R, kf, true);
+    }
     if (ok) {
       a.ctrl = ctrl;
       k_set<<<1, 1, 0, st>>>(ctrl, 0);
@@ -1198,6 +1309,11 @@ void forward_impl(const ForwardCall<T>& fc) {
                   else tmi_fwd_e<T, 4><<<gi, wblock, 0, q>>>(b, tf, pE.interior);
                 });
           });
+        } else if (fast3) {
+          if constexpr (sizeof(T) == 4) {
+            timed(KK_FWD_H, st, [&] { k3t_launch<false>(R, eq3, st, kmH, b, kf, ktg); });
+            timed(KK_FWD_E, st, [&] { k3t_launch<true>(R, eq3, st, kmE, b, kf, ktg); });
+          }
         } else {
           const dim3 g3((unsigned)kg.nblocks), b3(32, K3_WARPS);
           const dim3 gfr((kg.fr.cum[5] + kBlock - 1) / kBlock, (unsigned)g.nshot);
@@ -1220,6 +1336,16 @@ void forward_impl(const ForwardCall<T>& fc) {
         }
       };
       ok = run_loop(cm.nt, +1, ctrl, st, issue);
+      if (ok && fast3) {
+        // a staged-tile wait that ran out leaves its bit in the control block
+        int herr = 0;
+        ok = cuda_ok(cudaMemcpyAsync(&herr, &ctrl->error, sizeof(int), cudaMemcpyDeviceToHost, st), "error readback") &&
+             cuda_ok(cudaStreamSynchronize(st), "error readback");
+        if (ok && (herr & kErrWaitTimeout)) {
+          set_error("forward: a staged-tile copy did not arrive in time (device error bits %d)", herr);
+          ok = false;
+        }
+      }
       if (ok && tm2d) {
         k_unpack2d_pitch<T><<<2048, 256, 0, st>>>(tf.Ez, fc.Ez, (long long)g.nshot * g.NX, g.NY, tg.NYP);
         k_unpack2d_pitch<T><<<2048, 256, 0, st>>>(tf.Hx, fc.Hx, (long long)g.nshot * g.NX, g.NY, tg.NYP);
@@ -1762,9 +1888,10 @@ DGB_API void forward(DGB_FWD_PARAMS(float)) { DGB_FORWARD_BODY(float); }
 // forward() without device memory allocation: its scratch comes from the
 // static array g_noalloc_scratch (8 MiB per device) and its time-step
 // kernels are launched one by one.  See StaticScratch for the callers this
-// serves, the size limit and why overlapping calls race.  The first call on
-// a device does set-up (the scratch address lookup; on a new thread also the
-// library's stream and events): make it before any stream capture.
+// serves, the size limit and why overlapping calls race.  Every call looks up
+// the array's device address; the first call on a new thread also creates the
+// library's stream and events for it: make that first call before any stream
+// capture.
 template <typename T>
 static void forward_noalloc_entry(ForwardCall<T>& fc) {
   const int saved = g_opt.use_graph;
@@ -1855,6 +1982,29 @@ DGB_API int dgb_set_scratch_retention(long long bytes) {
                "dgb_set_scratch_retention: release threshold"))
     return -1;
   if (bytes == 0 && !cuda_ok(cudaMemPoolTrimTo(pool, 0), "dgb_set_scratch_retention: trim")) return -1;
+  return 0;
+}
+
+// Diagnostic: bytes in use in the current device's default stream-ordered
+// memory pool (the pool cudaMallocAsync draws on), and its high-water mark
+// since the last reset; reset_high != 0 first resets the mark to the current
+// use.  Returns 0, or -1 with the error.
+DGB_API int dgb_default_pool_usage(long long* used, long long* high, int reset_high) {
+  int dev = 0;
+  if (!cuda_ok(cudaGetDevice(&dev), "dgb_default_pool_usage: device")) return -1;
+  cudaMemPool_t pool;
+  if (!cuda_ok(cudaDeviceGetDefaultMemPool(&pool, dev), "dgb_default_pool_usage: pool")) return -1;
+  unsigned long long u = 0, h = 0;
+  if (reset_high) {
+    unsigned long long zero = 0;
+    if (!cuda_ok(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrUsedMemHigh, &zero), "dgb_default_pool_usage: reset"))
+      return -1;
+  }
+  if (!cuda_ok(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &u), "dgb_default_pool_usage: used") ||
+      !cuda_ok(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemHigh, &h), "dgb_default_pool_usage: high"))
+    return -1;
+  if (used) *used = (long long)u;
+  if (high) *high = (long long)h;
   return 0;
 }
 

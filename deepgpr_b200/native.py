@@ -104,6 +104,7 @@ SCALAR_SYMBOLS: Dict[str, Tuple[Tuple[str, ...], Optional[str]]] = {
     "dgb_history_bytes": (("int", "int", "int", "int", "long long", "int", "int", "int", "int"), "long long"),
     "dgb_check_fixed_division": (("float", "void*", "void*"), "int"),
     "dgb_set_scratch_retention": (("long long",), "int"),
+    "dgb_default_pool_usage": (("void*", "void*", "int"), "int"),
     "dgb_profile": (("int",), None),
     "dgb_launch_count": ((), "long long"),
     "dgb_profile_read": (("void*", "void*", "int"), "int"),
@@ -137,6 +138,17 @@ def set_scratch_retention(nbytes: int) -> None:
     lib = load_library()
     if lib.dgb_set_scratch_retention(int(nbytes)) != 0:
         raise NativeLibraryError(last_error(lib) or "dgb_set_scratch_retention failed")
+
+
+def default_pool_usage(reset_high: bool = False) -> Tuple[int, int]:
+    """(bytes in use, high-water mark) of the current device's default
+    stream-ordered memory pool; ``reset_high`` first resets the mark."""
+    lib = load_library()
+    used = ctypes.c_longlong(0)
+    high = ctypes.c_longlong(0)
+    if lib.dgb_default_pool_usage(ctypes.addressof(used), ctypes.addressof(high), int(bool(reset_high))) != 0:
+        raise NativeLibraryError(last_error(lib) or "dgb_default_pool_usage failed")
+    return int(used.value), int(high.value)
 
 
 def check_fixed_division(divisor: float) -> Tuple[int, int]:

@@ -146,9 +146,9 @@ void dgb_backward_f64(/* backward's parameters, float -> double */);
  * scratch (control block, source / receiver tables and bitmaps, the pitched
  * 2D working copy) is a static array of DGB_NOALLOC_SCRATCH_BYTES (8 MiB) per
  * device; a solve whose scratch does not fit is rejected through
- * deepgpr_last_error() before any time step runs.  The first call on a device
- * does set-up (it looks up the array's address; on a new thread it also
- * creates the library's stream and events): make it before any stream
+ * deepgpr_last_error() before any time step runs.  Every call looks up the
+ * array's device address; the first call on a new thread also creates the
+ * library's stream and events for that thread: make it before any stream
  * capture.  All calls on a device share the array, so overlapping calls (two
  * threads, or two streams) race. */
 #define DGB_NOALLOC_SCRATCH_BYTES 8388608
@@ -193,6 +193,12 @@ int dgb_check_fixed_division(float divisor, unsigned long long* mismatches, unsi
  * pool.  Affects every stream-ordered allocation of the process on that
  * device.  Returns 0, or -1 with deepgpr_last_error() set. */
 int dgb_set_scratch_retention(long long bytes);
+
+/* No counterpart in the reference (diagnostic).  Bytes in use in the current
+ * device's default stream-ordered memory pool (the pool cudaMallocAsync draws
+ * on) and its high-water mark; reset_high != 0 first resets the mark to the
+ * current use.  Returns 0, or -1 with deepgpr_last_error() set. */
+int dgb_default_pool_usage(long long* used, long long* high, int reset_high);
 
 /* Process-wide kernel timing (CUDA events around every time-step
  * kernel; graph replay is off while enabled).  dgb_profile(1) clears the
