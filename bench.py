@@ -69,6 +69,7 @@ def parse():
     ap.add_argument("--only-3d", action="store_true", help="print the north_star_3d object alone (profiling)")
     ap.add_argument("--nt-3d", type=int, default=40)
     ap.add_argument("--shape-3d", default="320,320,160", help="physical grid of the 3D measurement")
+    ap.add_argument("--pml-3d", type=int, default=10, help="CPML thickness of the 3D measurement")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--only-serving", action="store_true", help="print the serving object alone")
     ap.add_argument("--serving-requests", type=int, default=40)
@@ -348,14 +349,14 @@ def ours(args, rank, world, local):
 BYTES_PER_CELL_3D = {"forward": 72, "adjoint": 104}
 
 
-def north_star_3d(dev, shots=4, nt=40, warmup=1, steps=2, shape=(320, 320, 160)):
+def north_star_3d(dev, shots=4, nt=40, warmup=1, steps=2, shape=(320, 320, 160), pml=10):
     """3D order-4 forward + adjoint: kernel time split and HBM roofline fractions."""
     import deepgpr_b200 as dg
     from deepgpr_b200 import native
     from deepgpr_b200.synthetic import fwi_3d
 
     acq = fwi_3d(seed=1005, shape=shape, dx=0.015, sources_grid=(2, 2), receivers_grid=(32, 32), nt=nt, order=4)
-    common = dict(dx=acq.dx, dt=acq.dt, pmlthick=10, fdtd_order=4, mode=3)
+    common = dict(dx=acq.dx, dt=acq.dt, pmlthick=pml, fdtd_order=4, mode=3)
     src, rcv, wave = acq.sources.to(dev), acq.receivers.to(dev), acq.wavelet.to(dev)
     eps0, sig0 = acq.eps_r.to(dev), acq.sigma.to(dev)
 
@@ -382,7 +383,7 @@ def north_star_3d(dev, shots=4, nt=40, warmup=1, steps=2, shape=(320, 320, 160))
     torch.cuda.synchronize()
     prof = native.profile_read()
     native.profile(False)
-    ext = tuple(n + 20 for n in shape)
+    ext = tuple(n + 2 * pml for n in shape)
     cells = ext[0] * ext[1] * ext[2]
     units = cells * nt * acq.sources.shape[0] * steps
     peak, peak_kind = peaks()
@@ -549,7 +550,8 @@ def main():
         elif args.only_3d:
             if rank == 0:
                 shape = tuple(int(v) for v in args.shape_3d.split(","))
-                print(json.dumps(north_star_3d(torch.device("cuda", local), nt=args.nt_3d, shape=shape)), flush=True)
+                print(json.dumps(north_star_3d(torch.device("cuda", local), nt=args.nt_3d, shape=shape, pml=args.pml_3d)),
+                      flush=True)
         else:
             ours(args, rank, world, local)
     finally:
