@@ -74,6 +74,10 @@ def parse():
     ap.add_argument("--only-serving", action="store_true", help="print the serving object alone")
     ap.add_argument("--serving-requests", type=int, default=40)
     ap.add_argument("--cpu-sample", action="store_true", help="time the CPU backend sample alone (internal)")
+    ap.add_argument("--config3", action="store_true",
+                    help="3D order-8 gradient of the 200^3 config (8 shots, nt 2500, BF16 E+R history) with "
+                         "segment checkpointing; prints its own JSON object")
+    ap.add_argument("--config3-nt", type=int, default=2500)
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     return ap.parse_args()
 
@@ -403,6 +407,65 @@ def north_star_3d(dev, shots=4, nt=40, warmup=1, steps=2, shape=(320, 320, 160),
     }
 
 
+def config3_measure(dev, nt=2500, steps=1):
+    """Config 3 in full: 200^3 (+ CPML 10), 8 shots on a 2 x 4 surface grid, 24 x 24 receivers, order 8,
+    gradient mode 3, BF16 stored E^n and R^n histories (2.56 TB for nt 2500), so the gradient runs with
+    segment checkpointing and recompute; cell-updates/s counts forward + adjoint once each."""
+    import deepgpr_b200 as dg
+    from deepgpr_b200.synthetic import fwi_3d
+
+    acq = fwi_3d(seed=1003, shape=(200, 200, 200), dx=0.02, sources_grid=(2, 4), receivers_grid=(24, 24), nt=nt,
+                 order=8)
+    src, rcv, wave = acq.sources.to(dev), acq.receivers.to(dev), acq.wavelet.to(dev)
+    eps0, sig0 = acq.eps_r.to(dev), acq.sigma.to(dev)
+    plan_box = {}
+
+    def gradient():
+        from deepgpr_b200 import checkpoint as ck
+
+        real = ck.CheckpointedFDTDFunction.apply
+
+        def spy(cfg, tensors, plan, *rest):
+            plan_box["plan"] = plan
+            return real(cfg, tensors, plan, *rest)
+
+        ck.CheckpointedFDTDFunction.apply = spy
+        try:
+            eps = eps0.clone().requires_grad_(True)
+            sig = sig0.clone().requires_grad_(True)
+            out = dg.compute(dev, source_amplitudes=wave, source_location=src, receiver_location=rcv, eps_r=eps,
+                             sigma=sig, dx=acq.dx, dt=acq.dt, pmlthick=10, fdtd_order=8, mode=3,
+                             wavefield_storage_dtype=torch.bfloat16, wavefield_rhs_history="stored",
+                             checkpoint_segments="auto")
+            loss = (out[-1] ** 2).sum()
+            del out
+            loss.backward()
+        finally:
+            ck.CheckpointedFDTDFunction.apply = real
+        return loss.detach()
+
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        loss = gradient()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    cells = 220 ** 3
+    units = 2 * cells * nt * acq.sources.shape[0]
+    plan = plan_box.get("plan")
+    return {
+        "workload": "config 3: 3D order-8 gradient, 200^3 (ext 220^3), 8 shots, 24x24 receivers, mode 3, "
+                    f"BF16 E+R history, nt {nt}",
+        "ms_per_gradient": ms, "cell_updates_per_s": units / (ms / 1e3), "loss": float(loss),
+        "history_bytes_full": 2 * 3 * 2 * cells * nt * 8,
+        "plan": None if plan is None else {"shot_batch": plan.shot_batch, "segment_steps": plan.segment_steps,
+                                           "segments": plan.nsegments, "forward_passes": plan.forward_passes,
+                                           "peak_gib": round(plan.peak_bytes / 2**30, 1)},
+    }
+
+
 def serving_measure(dev, n=40, slots=8):
     """Config-4 stream: continuous-batching server (FP8) vs plain per-request launches (FP32)."""
     from deepgpr_b200.serving import SolveServer, percentile, run_plain
@@ -544,6 +607,9 @@ def main():
             print(json.dumps(cpu_sample(args.shots, args.cpu_budget)), flush=True)
         elif args.impl == "reference":
             reference(args, rank, world)
+        elif args.config3:
+            if rank == 0:
+                print(json.dumps(config3_measure(torch.device("cuda", local), nt=args.config3_nt)), flush=True)
         elif args.only_serving:
             if rank == 0:
                 print(json.dumps(serving_measure(torch.device("cuda", local), n=args.serving_requests)), flush=True)

@@ -143,7 +143,7 @@ class CheckpointedFDTDFunction(torch.autograd.Function):
             args = forward_arguments(seg, tensors, states, empty, empty, rx, wave[:, t0:t1].contiguous(), stype,
                                      False)
             native.invoke(cfg.entry[0], args, fdtd_order=cfg.fdtd_order, stream=torch.cuda.current_stream(dev),
-                          acc64=cfg.acc64)
+                          acc64=cfg.acc64, chunk=cfg.chunk, tuning=cfg.tuning)
             receivers[:, t0:t1] = rx
         ctx.cfg, ctx.tensors, ctx.plan = cfg, tensors, plan
         ctx.wave = wave
@@ -202,7 +202,8 @@ class CheckpointedFDTDFunction(torch.autograd.Function):
                     rx = torch.empty((nb, t1 - t0, cfg.nrx), device=dev, dtype=dtype)
                     args = forward_arguments(seg, bt, cur, empty, empty, rx, wave[:, t0:t1].contiguous(), st_none,
                                              False)
-                    native.invoke(cfg.entry[0], args, fdtd_order=cfg.fdtd_order, stream=stream, acc64=cfg.acc64)
+                    native.invoke(cfg.entry[0], args, fdtd_order=cfg.fdtd_order, stream=stream, acc64=cfg.acc64,
+                                  chunk=cfg.chunk, tuning=cfg.tuning)
                 del cur
             lam = [t[b0:b1].clone() if t.numel() else t for t in lambdas] if plan.shot_batch < cfg.nstep else lambdas
             for k in range(len(bounds) - 1, -1, -1):
@@ -221,13 +222,15 @@ class CheckpointedFDTDFunction(torch.autograd.Function):
                 ws = wave[:, t0:t1].contiguous()
                 fargs = forward_arguments(seg, bt, cur, e_saved, r_saved, rx, ws, st_hist if save_model else st_none,
                                           save_model)
-                native.invoke(cfg.entry[0], fargs, fdtd_order=cfg.fdtd_order, stream=stream, acc64=cfg.acc64)
+                native.invoke(cfg.entry[0], fargs, fdtd_order=cfg.fdtd_order, stream=stream, acc64=cfg.acc64,
+                              chunk=cfg.chunk, tuning=cfg.tuning)
                 del cur, rx
                 gsrc = torch.zeros((ctx.source_shape[0], t1 - t0), device=dev, dtype=dtype) if want_src else empty.to(dtype)
                 dg = data_grad[b0:b1, t0:t1].contiguous()
                 bargs = backward_arguments(seg, bt, lam, e_saved, r_saved, dg, gsrc, grad_eps, grad_sig, ctx.want,
                                            st_hist if save_model else st_none)
-                native.invoke(cfg.entry[1], bargs, fdtd_order=cfg.fdtd_order, stream=stream, acc64=cfg.acc64)
+                native.invoke(cfg.entry[1], bargs, fdtd_order=cfg.fdtd_order, stream=stream, acc64=cfg.acc64,
+                              chunk=cfg.chunk, tuning=cfg.tuning)
                 del e_saved, r_saved
                 if want_src:
                     grad_src.view(grad_src.shape[0], -1)[:, t0:t1] += gsrc

@@ -51,6 +51,11 @@ struct ThreadOptions {
   int chunk = 16;         // time steps per launch chunk
   int use_graph = 1;      // capture a chunk into a CUDA graph and replay it
   int order_override = 0; // per-thread FDTD order (0: use the global)
+  // launch-shape choices of the autotuner (0 / -1: the built-in heuristics)
+  int tm_chunks = 0;       // 2D: row chunks of the interior rectangles
+  int tm_frame_rows = 0;   // 2D: rows per frame warp chunk
+  int k3_xchunks = 0;      // 3D: x chunks of the z-streamed and staged kernels
+  int tma = -1;            // 3D forward: staged (TMA) kernels 1, z-streamed 0, -1 DEEPGPR_B200_TMA
 };
 thread_local ThreadOptions g_opt;
 
@@ -234,18 +239,72 @@ struct StaticScratch {
   }
 };
 
-// Sorted point table (see PointTable in fdtd_common.cuh) built on the host
-// from the caller's (nshot, npts, 3) int32 locations.
+// ---------------------------------------------------------------------------
+// Source and receiver point sets of one call, built together: one
+// device->host read of both location arrays and one synchronisation, the
+// tables, per-shot bitmaps and per-(shot, x) row flags built on the host, and
+// one host->device copy of everything.  The copy leaves from a per-thread
+// pinned staging buffer (its previous upload is awaited before the buffer is
+// rewritten), so no further synchronisation is needed; the no-allocation
+// entry point copies from pageable memory and synchronises instead.
+// ---------------------------------------------------------------------------
+struct PinnedStage {
+  int device = -1;
+  unsigned char* buf = nullptr;
+  size_t cap = 0;
+  cudaEvent_t done = nullptr;
+  bool pending = false;
+};
+thread_local std::vector<PinnedStage> g_stages;
+
+PinnedStage* pinned_stage(size_t bytes) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  PinnedStage* ps = nullptr;
+  for (auto& x : g_stages)
+    if (x.device == dev) ps = &x;
+  if (!ps) {
+    g_stages.push_back(PinnedStage());
+    ps = &g_stages.back();
+    ps->device = dev;
+    if (cudaEventCreateWithFlags(&ps->done, cudaEventDisableTiming) != cudaSuccess) return nullptr;
+  }
+  if (ps->pending) {
+    cudaEventSynchronize(ps->done);
+    ps->pending = false;
+  }
+  if (ps->cap < bytes) {
+    // grown to the next power of two (at least 1 MiB); an outgrown buffer is
+    // kept, not freed: freeing pinned memory synchronises the whole device,
+    // which would stall every other solve in flight
+    size_t want = size_t(1) << 20;
+    while (want < bytes) want <<= 1;
+    unsigned char* buf = nullptr;
+    if (cudaHostAlloc(reinterpret_cast<void**>(&buf), want, cudaHostAllocDefault) != cudaSuccess) return nullptr;
+    ps->buf = buf;
+    ps->cap = want;
+  }
+  return ps;
+}
+
 template <typename Alloc>
-bool build_table(const int* loc, int nshot, int npts, const Grid& g, cudaStream_t st, Alloc& scratch,
-                 PointTable* out, const char* what, int err_code) {
-  out->n = 0;
-  out->cells = out->off = out->shot = out->idx = nullptr;
-  if (npts <= 0 || nshot <= 0 || loc == nullptr) return true;
+struct UploadsPageable : std::false_type {};
+template <>
+struct UploadsPageable<StaticScratch> : std::true_type {};
+
+// One point set's host-side image: the sorted table, bitmaps and row flags
+// (see PointTable / PointSet).
+struct HostPointSet {
+  std::vector<int> table;          // cells | off | shot | idx
+  int unique = 0, n = 0;
+  std::vector<unsigned> bits;      // nshot * words_per_shot
+  std::vector<unsigned char> rows; // nshot * NX
+  std::vector<char> any;           // NX: some shot has a point there
+};
+
+bool host_pointset(const int* h, int nshot, int npts, const Grid& g, const char* what, bool want_rows,
+                   HostPointSet& out) {
   const size_t n = (size_t)nshot * npts;
-  std::vector<int> h(n * 3);
-  if (!cuda_ok(cudaMemcpyAsync(h.data(), loc, n * 3 * sizeof(int), cudaMemcpyDefault, st), what)) return false;
-  if (!cuda_ok(cudaStreamSynchronize(st), what)) return false;
   struct E {
     int cell, shot, idx;
   };
@@ -254,9 +313,8 @@ bool build_table(const int* loc, int nshot, int npts, const Grid& g, cudaStream_
     for (int m = 0; m < npts; ++m) {
       const int* p = &h[((size_t)s * npts + m) * 3];
       if (p[0] < 0 || p[0] >= g.NX || p[1] < 0 || p[1] >= g.NY || p[2] < 0 || p[2] >= g.NZ) {
-        set_error("%s location (%d, %d, %d) of shot %d, index %d is outside the field grid (%d, %d, %d)", what,
-                  p[0], p[1], p[2], s, m, g.NX, g.NY, g.NZ);
-        (void)err_code;
+        set_error("%s location (%d, %d, %d) of shot %d, index %d is outside the field grid (%d, %d, %d)", what, p[0],
+                  p[1], p[2], s, m, g.NX, g.NY, g.NZ);
         return false;
       }
       ent[(size_t)s * npts + m] = E{p[0] * g.sx + p[1] * g.NZ + p[2], s, m};
@@ -276,74 +334,119 @@ bool build_table(const int* loc, int nshot, int npts, const Grid& g, cudaStream_
     idx[e] = ent[e].idx;
   }
   off.push_back((int)n);
-  const size_t U = cells.size();
-  std::vector<int> packed;
-  packed.reserve(U + (U + 1) + 2 * n);
-  packed.insert(packed.end(), cells.begin(), cells.end());
-  packed.insert(packed.end(), off.begin(), off.end());
-  packed.insert(packed.end(), shot.begin(), shot.end());
-  packed.insert(packed.end(), idx.begin(), idx.end());
-  int* d = scratch.template get<int>(packed.size() * sizeof(int));
-  if (!d) return false;
-  if (!cuda_ok(cudaMemcpyAsync(d, packed.data(), packed.size() * sizeof(int), cudaMemcpyHostToDevice, st), what))
-    return false;
-  // the pageable source must stay valid until the copy ran
-  if (!cuda_ok(cudaStreamSynchronize(st), what)) return false;
-  out->cells = d;
-  out->off = d + U;
-  out->shot = d + U + (U + 1);
-  out->idx = d + U + (U + 1) + n;
-  out->n = (int)U;
-  return true;
-}
-
-// Table plus per-shot membership bitmaps.
-template <typename Alloc>
-bool build_pointset(const int* loc, int nshot, int npts, const Grid& g, cudaStream_t st, Alloc& scratch,
-                    PointSet* ps, PointTable* tb_out, const char* what, int err_code,
-                    const unsigned char** rows_out = nullptr, std::vector<char>* any_rows = nullptr) {
-  if (rows_out) *rows_out = nullptr;
-  ps->tb.n = 0;
-  ps->tb.cells = ps->tb.off = ps->tb.shot = ps->tb.idx = nullptr;
-  ps->bits = nullptr;
-  ps->words_per_shot = (g.cells + 31) / 32;
-  if (!build_table(loc, nshot, npts, g, st, scratch, &ps->tb, what, err_code)) return false;
-  if (tb_out) *tb_out = ps->tb;
-  if (ps->tb.n == 0) return true;
-  // rebuild the bitmap on the host from the same (validated) locations
-  const size_t n = (size_t)nshot * npts;
-  std::vector<int> h(n * 3);
-  if (!cuda_ok(cudaMemcpyAsync(h.data(), loc, n * 3 * sizeof(int), cudaMemcpyDefault, st), what)) return false;
-  if (!cuda_ok(cudaStreamSynchronize(st), what)) return false;
-  std::vector<unsigned> bits((size_t)nshot * ps->words_per_shot, 0u);
+  out.unique = (int)cells.size();
+  out.n = (int)n;
+  out.table.clear();
+  out.table.reserve(cells.size() + off.size() + 2 * n);
+  out.table.insert(out.table.end(), cells.begin(), cells.end());
+  out.table.insert(out.table.end(), off.begin(), off.end());
+  out.table.insert(out.table.end(), shot.begin(), shot.end());
+  out.table.insert(out.table.end(), idx.begin(), idx.end());
+  const int words = (g.cells + 31) / 32;
+  out.bits.assign((size_t)nshot * words, 0u);
+  out.any.assign(g.NX, 0);
+  if (want_rows) out.rows.assign((size_t)nshot * g.NX, 0);
   for (int s = 0; s < nshot; ++s)
     for (int m = 0; m < npts; ++m) {
       const int* p = &h[((size_t)s * npts + m) * 3];
       const int c = p[0] * g.sx + p[1] * g.NZ + p[2];
-      bits[(size_t)s * ps->words_per_shot + (c >> 5)] |= 1u << (c & 31);
+      out.bits[(size_t)s * words + (c >> 5)] |= 1u << (c & 31);
+      out.any[p[0]] = 1;
+      if (want_rows) out.rows[(size_t)s * g.NX + p[0]] = 1;
     }
-  unsigned* d = scratch.template get<unsigned>(bits.size() * sizeof(unsigned));
-  if (!d) return false;
-  if (!cuda_ok(cudaMemcpyAsync(d, bits.data(), bits.size() * sizeof(unsigned), cudaMemcpyHostToDevice, st), what))
+  return true;
+}
+
+// Builds the source set (when src_loc is given) and the receiver set (when
+// rcv_loc is given) of a call.  rows_*: per (shot, x index) flags on the
+// device, the plane holds a point of the shot; any_*: host mask over x
+// indices, some shot has a point there.
+template <typename Alloc>
+bool build_points(const int* src_loc, int nsrc, const int* rcv_loc, int nrcv, const Grid& g, cudaStream_t st,
+                  Alloc& scratch, PointSet* sps, PointTable* stb, PointSet* rps, PointTable* rtb,
+                  const unsigned char** src_rows, const unsigned char** rcv_rows, std::vector<char>* src_any,
+                  std::vector<char>* rcv_any) {
+  PointSet* ps[2] = {sps, rps};
+  PointTable* tbo[2] = {stb, rtb};
+  const int* loc[2] = {src_loc, rcv_loc};
+  const int np[2] = {nsrc, nrcv};
+  const unsigned char** rows_out[2] = {src_rows, rcv_rows};
+  std::vector<char>* any_out[2] = {src_any, rcv_any};
+  const char* what[2] = {"source", "receiver"};
+  bool use[2];
+  std::vector<int> h[2];
+  for (int q = 0; q < 2; ++q) {
+    if (rows_out[q]) *rows_out[q] = nullptr;
+    if (ps[q]) {
+      ps[q]->tb.n = 0;
+      ps[q]->tb.cells = ps[q]->tb.off = ps[q]->tb.shot = ps[q]->tb.idx = nullptr;
+      ps[q]->bits = nullptr;
+      ps[q]->words_per_shot = (g.cells + 31) / 32;
+    }
+    if (tbo[q]) *tbo[q] = PointTable{nullptr, nullptr, nullptr, nullptr, 0};
+    use[q] = ps[q] != nullptr && loc[q] != nullptr && np[q] > 0 && g.nshot > 0;
+    if (use[q]) {
+      h[q].resize((size_t)g.nshot * np[q] * 3);
+      if (!cuda_ok(cudaMemcpyAsync(h[q].data(), loc[q], h[q].size() * sizeof(int), cudaMemcpyDefault, st), what[q]))
+        return false;
+    }
+  }
+  if (!use[0] && !use[1]) return true;
+  if (!cuda_ok(cudaStreamSynchronize(st), "point locations")) return false;
+  HostPointSet hs[2];
+  size_t off[2][3], total = 0;
+  auto reserve = [&](size_t bytes) {
+    const size_t o = (total + 255) & ~size_t(255);
+    total = o + bytes;
+    return o;
+  };
+  for (int q = 0; q < 2; ++q) {
+    if (!use[q]) continue;
+    if (!host_pointset(h[q].data(), g.nshot, np[q], g, what[q], rows_out[q] != nullptr, hs[q])) return false;
+    off[q][0] = reserve(hs[q].table.size() * sizeof(int));
+    off[q][1] = reserve(hs[q].bits.size() * sizeof(unsigned));
+    off[q][2] = reserve(hs[q].rows.size());
+  }
+  unsigned char* dev = scratch.template get<unsigned char>(total);
+  if (!dev) return false;
+  std::vector<unsigned char> pageable;
+  PinnedStage* stage = nullptr;
+  unsigned char* host = nullptr;
+  if (UploadsPageable<Alloc>::value) {
+    pageable.resize(total);
+    host = pageable.data();
+  } else {
+    stage = pinned_stage(total);
+    if (!stage) {
+      set_error("point tables: pinned staging buffer of %zu bytes could not be allocated", total);
+      return false;
+    }
+    host = stage->buf;
+  }
+  for (int q = 0; q < 2; ++q) {
+    if (!use[q]) continue;
+    memcpy(host + off[q][0], hs[q].table.data(), hs[q].table.size() * sizeof(int));
+    memcpy(host + off[q][1], hs[q].bits.data(), hs[q].bits.size() * sizeof(unsigned));
+    if (!hs[q].rows.empty()) memcpy(host + off[q][2], hs[q].rows.data(), hs[q].rows.size());
+  }
+  if (!cuda_ok(cudaMemcpyAsync(dev, host, total, cudaMemcpyHostToDevice, st), "point tables upload")) return false;
+  if (stage) {
+    cudaEventRecord(stage->done, st);
+    stage->pending = true;
+  } else if (!cuda_ok(cudaStreamSynchronize(st), "point tables upload")) {
     return false;
-  if (any_rows) {
-    // host mask over x indices: some shot has a point there
-    any_rows->assign(g.NX, 0);
-    for (size_t m = 0; m < n; ++m) (*any_rows)[h[m * 3]] = 1;
   }
-  if (rows_out) {
-    // per (shot, x index) flag: the row/plane holds a point of the shot
-    std::vector<unsigned char> rows((size_t)nshot * g.NX, 0);
-    for (int s = 0; s < nshot; ++s)
-      for (int m = 0; m < npts; ++m) rows[(size_t)s * g.NX + h[((size_t)s * npts + m) * 3]] = 1;
-    unsigned char* dr = scratch.template get<unsigned char>(rows.size());
-    if (!dr) return false;
-    if (!cuda_ok(cudaMemcpyAsync(dr, rows.data(), rows.size(), cudaMemcpyHostToDevice, st), what)) return false;
-    if (!cuda_ok(cudaStreamSynchronize(st), what)) return false;
-    *rows_out = dr;
+  for (int q = 0; q < 2; ++q) {
+    if (!use[q]) continue;
+    const int U = hs[q].unique, n = hs[q].n;
+    int* t = reinterpret_cast<int*>(dev + off[q][0]);
+    PointTable tb{t, t + U, t + U + (U + 1), t + U + (U + 1) + n, U};
+    ps[q]->tb = tb;
+    ps[q]->bits = reinterpret_cast<const unsigned*>(dev + off[q][1]);
+    if (tbo[q]) *tbo[q] = tb;
+    if (rows_out[q]) *rows_out[q] = dev + off[q][2];
+    if (any_out[q]) *any_out[q] = hs[q].any;
   }
-  if (!cuda_ok(cudaStreamSynchronize(st), what)) return false;
-  ps->bits = d;
   return true;
 }
 
@@ -467,7 +570,7 @@ TmPlan tm_plan(const TmGeom& base, const Grid& g, int kind, int R, const TmFaces
   const auto xg = complement(g.NX, xl);
   const auto mid = complement(g.NX, rows);
   const bool fits = 2 * xl.size() + 2 * xg.size() + mid.size() <= (size_t)kTmMaxRects;
-  const int frame_xc = 8, corner_xc = 2;
+  const int frame_xc = g_opt.tm_frame_rows > 0 ? g_opt.tm_frame_rows : 8, corner_xc = 2;
   if (!rows.empty() && thi > tlo && fits) {
     const int n128 = (thi - tlo + 3) / 4;
     int nrows = 0;
@@ -476,6 +579,7 @@ TmPlan tm_plan(const TmGeom& base, const Grid& g, int kind, int R, const TmFaces
     const long long resident = (long long)sm_count() * iblocks * TM_WARPS;
     long long chunks = std::max<long long>(1, resident / per);
     chunks = std::min<long long>(chunks, std::max(1, nrows / 16));
+    if (g_opt.tm_chunks > 0) chunks = std::min(g_opt.tm_chunks, std::max(1, nrows));
     const int xc = (int)((nrows + chunks - 1) / chunks);
     for (auto& r : rows) tm_add_rect(pl.interior, g.nshot, tlo, n128, 4 * TMW, r.first, r.second, xc);
     pl.interior.col1 = thi * TMW;
@@ -718,6 +822,7 @@ K3Geom k3_layout(const Grid& g) {
       best = n;
     }
   }
+  if (g_opt.k3_xchunks > 0) best = std::min(g_opt.k3_xchunks, g.NX);
   kg.xc = (g.NX + best - 1) / best;
   kg.nchunk = (g.NX + kg.xc - 1) / kg.xc;
   kg.nblocks = per * kg.nchunk;
@@ -888,16 +993,43 @@ bool launch_coeffs(const Common<T>& cm, cudaStream_t st) {
   return cuda_ok(cudaGetLastError(), "coefficient kernel");
 }
 
+// Instantiated time-loop graphs kept across calls, per thread, device and
+// direction: a call captures its chunk and updates the kept executable in
+// place (cudaGraphExecUpdate) when the captured topology is the same, which
+// spares the instantiation; otherwise it instantiates anew.
+struct GraphCache {
+  int device, dir;
+  cudaGraphExec_t exec;
+};
+thread_local std::vector<GraphCache> g_graphs;
+
+cudaGraphExec_t* cached_exec(int dir) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  for (auto& c : g_graphs)
+    if (c.device == dev && c.dir == dir) return &c.exec;
+  g_graphs.push_back(GraphCache{dev, dir, nullptr});
+  return &g_graphs.back().exec;
+}
+
+struct NoHook {
+  bool operator()(int, int, int) const { return true; }
+};
+
 // Issue `steps` time steps through `issue(k)` in chunks, with graph replay.
-template <typename Issue>
-bool run_loop(int steps, int dir, Control* ctrl, cudaStream_t st, Issue issue) {
+// hook(t, K, phase) runs before (phase 0) and after (phase 1) the chunk of
+// steps t .. t+K-1 is issued (host-side staging around chunks).
+template <typename Issue, typename Hook = NoHook>
+bool run_loop(int steps, int dir, Control* ctrl, cudaStream_t st, Issue issue, Hook hook = Hook()) {
   const int chunk = std::max(1, g_opt.chunk);
   cudaGraphExec_t exec = nullptr;
+  bool owned = false;   // exec is not the kept one: destroy it at the end
   long long per_replay = 0;
   bool ok = true;
   int t = 0;
   while (ok && t < steps) {
     const int K = std::min(chunk, steps - t);
+    if (!hook(t, K, 0)) return false;
     if (g_opt.use_graph && !g_prof.on && K == chunk && steps >= 2 * chunk) {
       if (!exec) {
         cudaGraph_t graph = nullptr;
@@ -912,7 +1044,22 @@ bool run_loop(int steps, int dir, Control* ctrl, cudaStream_t st, Issue issue) {
         cudaError_t e2 = cudaStreamEndCapture(st, &graph);
         ok = cuda_ok(e1, "capture launch") && cuda_ok(e2, "end capture");
         if (!ok) break;
-        ok = cuda_ok(cudaGraphInstantiate(&exec, graph, 0), "graph instantiate");
+        cudaGraphExec_t* kept = cached_exec(dir);
+        if (kept && *kept) {
+          cudaGraphExecUpdateResultInfo info;
+          if (cudaGraphExecUpdate(*kept, graph, &info) == cudaSuccess) {
+            exec = *kept;
+          } else {
+            cudaGetLastError();
+            cudaGraphExecDestroy(*kept);
+            *kept = nullptr;
+          }
+        }
+        if (!exec) {
+          ok = cuda_ok(cudaGraphInstantiate(&exec, graph, 0), "graph instantiate");
+          if (ok && kept) *kept = exec;
+          else owned = ok;
+        }
         cudaGraphDestroy(graph);
         if (!ok) break;
       }
@@ -925,11 +1072,116 @@ bool run_loop(int steps, int dir, Control* ctrl, cudaStream_t st, Issue issue) {
       ok = cuda_ok(cudaGetLastError(), "time-step launch");
       if (g_prof.on) harvest_profile();
     }
+    if (ok && !hook(t, K, 1)) ok = false;
     t += K;
   }
-  if (exec) cudaGraphExecDestroy(exec);
+  if (exec && owned) cudaGraphExecDestroy(exec);
   return ok;
 }
+
+// ---------------------------------------------------------------------------
+// Asynchronous history offload (use_async_offload): a history that lives in
+// pinned host memory is written and read by the kernels through a pair of
+// device ring buffers.  Every kernel indexes a history as
+//   base + q * comp_stride + slot * frame + (cell offset),
+// so a chunk of time steps touching the saved slots s0 .. s1-1 is pointed at
+// ring buffer b with base = ring[b] - s0 * frame and comp_stride =
+// ring_slots * frame; no kernel knows about the ring.  A copy stream moves
+// each chunk's slots between the ring and the host while the next chunk
+// computes: forward, the copy of chunk c runs beside chunk c+1 and buffer b
+// is rewritten by chunk c+2 only after its copy ended; backward, the slots of
+// chunk c+1 (and c+2) are staged ahead of their use.
+// ---------------------------------------------------------------------------
+bool is_host_memory(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeHost;
+}
+
+struct HistRing {
+  bool on = false;
+  int S = 1, nt = 0, nt_saved = 0, ncomp = 1, slots = 0, extra = 0;
+  size_t frame_bytes = 0;       // one saved step of one component, all shots
+  long long frame_elems = 0;
+  char* host[2] = {nullptr, nullptr};   // E, R host histories (R: nullptr when not offloaded)
+  char* ring[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};   // [history][buffer]
+  cudaStream_t copy = nullptr;
+  cudaEvent_t done[2] = {nullptr, nullptr}, work[2] = {nullptr, nullptr};
+  bool pending[2] = {false, false};
+
+  // slots of forward chunk [t, t+K) and of reverse chunk (steps nt-1-t down to nt-t-K)
+  void fwd_slots(int t, int K, int& s0, int& s1) const {
+    s0 = (t + S - 1) / S;
+    s1 = (t + K + S - 1) / S;
+  }
+  void bwd_slots(int t, int K, int& s0, int& s1) const {
+    const int lo = std::max(0, nt - t - K), hi = nt - 1 - t;
+    s0 = (lo + S - 1) / S;
+    s1 = std::min(nt_saved, hi / S + 1 + extra);
+  }
+  template <typename Alloc>
+  bool setup(Alloc& scratch, cudaStream_t st, void* e_host, void* r_host, int S_, int nt_, int nt_saved_, int ncomp_,
+             long long frame, int elem, int chunk, int extra_) {
+    S = S_;
+    nt = nt_;
+    nt_saved = nt_saved_;
+    ncomp = ncomp_;
+    extra = extra_;
+    frame_elems = frame;
+    frame_bytes = (size_t)frame * elem;
+    slots = (chunk + S - 1) / S + 1 + extra;
+    host[0] = static_cast<char*>(e_host);
+    host[1] = static_cast<char*>(r_host);
+    for (int h = 0; h < 2; ++h) {
+      if (!host[h]) continue;
+      for (int b = 0; b < 2; ++b) {
+        ring[h][b] = scratch.template get<char>((size_t)ncomp * slots * frame_bytes);
+        if (!ring[h][b]) return false;
+      }
+    }
+    if (!cuda_ok(cudaStreamCreateWithFlags(&copy, cudaStreamNonBlocking), "offload copy stream")) return false;
+    for (int b = 0; b < 2; ++b)
+      if (!cuda_ok(cudaEventCreateWithFlags(&done[b], cudaEventDisableTiming), "offload event") ||
+          !cuda_ok(cudaEventCreateWithFlags(&work[b], cudaEventDisableTiming), "offload event"))
+        return false;
+    on = true;
+    (void)st;
+    return true;
+  }
+  // device base of history h for a chunk whose first slot is s0 in buffer b
+  void* base(int h, int b, int s0) const { return ring[h][b] - (long long)s0 * (long long)frame_bytes; }
+  long long comp_stride() const { return (long long)slots * frame_elems; }
+  // copies slots s0 .. s1-1 of buffer b to (dir > 0) or from (dir < 0) the host, on the copy stream
+  bool move(int b, int s0, int s1, bool to_host) {
+    if (s1 <= s0) return true;
+    for (int h = 0; h < 2; ++h) {
+      if (!host[h]) continue;
+      for (int q = 0; q < ncomp; ++q) {
+        char* hp = host[h] + ((long long)q * nt_saved + s0) * (long long)frame_bytes;
+        char* dp = ring[h][b] + (long long)q * slots * (long long)frame_bytes;
+        const size_t n = (size_t)(s1 - s0) * frame_bytes;
+        const cudaError_t e = to_host ? cudaMemcpyAsync(hp, dp, n, cudaMemcpyDeviceToHost, copy)
+                                      : cudaMemcpyAsync(dp, hp, n, cudaMemcpyHostToDevice, copy);
+        if (!cuda_ok(e, "history offload copy")) return false;
+      }
+    }
+    return true;
+  }
+  void release() {
+    if (copy) cudaStreamSynchronize(copy);
+    for (int b = 0; b < 2; ++b) {
+      if (done[b]) cudaEventDestroy(done[b]);
+      if (work[b]) cudaEventDestroy(work[b]);
+    }
+    if (copy) cudaStreamDestroy(copy);
+    copy = nullptr;
+  }
+  ~HistRing() { release(); }
+};
 
 // ---------------------------------------------------------------------------
 // TMA-staged 3D forward kernels (fdtd_3d_fast.cuh): launch geometry, tensor
@@ -944,7 +1196,7 @@ bool env_flag(const char* name) {
 // DEEPGPR_B200_TMA=1, the single-face CPML form (or none), TMA plane
 // coordinates inside int32, and the driver's tensor-map encoder available.
 bool k3t_usable(const Grid& g, const int* p, bool has_cpml) {
-  if (!env_flag("DEEPGPR_B200_TMA")) return false;
+  if (g_opt.tma == 0 || (g_opt.tma < 0 && !env_flag("DEEPGPR_B200_TMA"))) return false;
   if (has_cpml && !k3_cpml_single(g, p)) return false;
   if ((long long)g.nshot * g.NX >= (1LL << 31)) return false;
   return encode_tiled_fn() != nullptr;
@@ -979,6 +1231,7 @@ K3TGeom k3t_layout(const Grid& g, int zp, int R) {
       best = n;
     }
   }
+  if (g_opt.k3_xchunks > 0) best = std::min(g_opt.k3_xchunks, g.NX);
   tg.xc = (g.NX + best - 1) / best;
   tg.nchunk = (g.NX + tg.xc - 1) / tg.xc;
   tg.nblocks = per * tg.nchunk;
@@ -1170,12 +1423,11 @@ void forward_impl(const ForwardCall<T>& fc) {
     // sources of an invalid component inject nothing (deepgpr_cpu.c:650)
     std::vector<char> src_any, rcv_any;
     const unsigned char *src_rows = nullptr, *rcv_rows = nullptr;
-    if (ok && fc.src_comp >= 0 && fc.src_comp <= 2)
-      ok = build_pointset(fc.src_loc, g.nshot, fc.nsrc, g, st, scratch, &P.src, &a.src, "source", kErrSourceRange,
-                          &src_rows, tm2d ? &src_any : nullptr);
-    if (ok)
-      ok = build_pointset(fc.rx_loc, g.nshot, fc.nrx, g, st, scratch, &P.rcv, &a.rcv, "receiver", kErrReceiverRange,
-                          &rcv_rows, tm2d ? &rcv_any : nullptr);
+    if (ok) {
+      const bool src_on = fc.src_comp >= 0 && fc.src_comp <= 2;
+      ok = build_points(src_on ? fc.src_loc : nullptr, fc.nsrc, fc.rx_loc, fc.nrx, g, st, scratch, &P.src, &a.src,
+                        &P.rcv, &a.rcv, &src_rows, &rcv_rows, tm2d ? &src_any : nullptr, tm2d ? &rcv_any : nullptr);
+    }
     tg.src_rows = src_rows;
     tg.rcv_rows = rcv_rows;
     // rows with a source or receiver of any shot go to the general (frame) kernels
@@ -1335,7 +1587,50 @@ void forward_impl(const ForwardCall<T>& fc) {
           });
         }
       };
-      ok = run_loop(cm.nt, +1, ctrl, st, issue);
+      // host-resident histories (use_async_offload): device rings and a copy stream
+      HistRing hr;
+      const ThreadOptions saved_opt = g_opt;
+      const bool off_e = history && is_host_memory(fc.E_saved);
+      const bool off_r = keep_r && is_host_memory(fc.R_saved);
+      if (ok && (off_e || off_r)) {
+        if (kind == kFP8) {
+          set_error("forward: FP8 histories stay on the device (no offload)");
+          ok = false;
+        } else {
+          g_opt.use_graph = 0;   // the ring base changes from chunk to chunk
+          g_opt.chunk = std::max(g_opt.chunk, 32);
+          ok = hr.setup(scratch, st, off_e ? fc.E_saved : nullptr, off_r ? fc.R_saved : nullptr, cm.S, cm.nt,
+                        a.nt_saved, ncomp, a.frame, hist_elem_bytes(kind), g_opt.chunk, 0);
+        }
+      }
+      const int clen = std::max(1, g_opt.chunk);
+      auto fhook = [&](int t, int K, int phase) -> bool {
+        if (!hr.on) return true;
+        int s0, s1;
+        hr.fwd_slots(t, K, s0, s1);
+        const int b = (t / clen) & 1;
+        if (phase == 0) {
+          if (hr.pending[b] && !cuda_ok(cudaStreamWaitEvent(st, hr.done[b], 0), "offload wait")) return false;
+          if (hr.host[0]) a.E_saved = hr.base(0, b, s0);
+          if (hr.host[1]) a.R_saved = hr.base(1, b, s0);
+          a.comp_stride = hr.comp_stride();
+          return true;
+        }
+        if (!cuda_ok(cudaEventRecord(hr.work[b], st), "offload event") ||
+            !cuda_ok(cudaStreamWaitEvent(hr.copy, hr.work[b], 0), "offload wait") || !hr.move(b, s0, s1, true))
+          return false;
+        hr.pending[b] = true;
+        return cuda_ok(cudaEventRecord(hr.done[b], hr.copy), "offload event");
+      };
+      if (ok) ok = run_loop(cm.nt, +1, ctrl, st, issue, fhook);
+      if (hr.on) {
+        for (int b = 0; b < 2; ++b)
+          if (hr.pending[b]) cudaStreamWaitEvent(st, hr.done[b], 0);
+        a.E_saved = fc.E_saved;
+        a.R_saved = fc.R_saved;
+        a.comp_stride = (long long)a.nt_saved * a.frame;
+      }
+      g_opt = saved_opt;
       if (ok && fast3) {
         // a staged-tile wait that ran out leaves its bit in the control block
         int herr = 0;
@@ -1566,13 +1861,13 @@ void backward_impl(const BackwardCall<T>& bc) {
       a.srcv = scratch.get<T>((size_t)g.nshot * bc.nsrc * sizeof(T));
       ok = a.srcv != nullptr;
       if (ok) cudaMemsetAsync(a.srcv, 0, (size_t)g.nshot * bc.nsrc * sizeof(T), st);
-      if (ok)
-        ok = build_pointset(bc.src_loc, g.nshot, bc.nsrc, g, st, scratch, &P.src, &a.src, "source", kErrSourceRange,
-                            &src_rows, tm2d ? &src_any : nullptr);
     }
-    if (ok && bc.rx_comp >= 0 && bc.rx_comp <= 2)
-      ok = build_pointset(bc.rx_loc, g.nshot, bc.ndata, g, st, scratch, &P.rcv, &a.rcv, "receiver", kErrReceiverRange,
-                          &rcv_rows, tm2d ? &rcv_any : nullptr);
+    if (ok) {
+      const bool rx_on = bc.rx_comp >= 0 && bc.rx_comp <= 2;
+      ok = build_points(a.want_src ? bc.src_loc : nullptr, bc.nsrc, rx_on ? bc.rx_loc : nullptr, bc.ndata, g, st,
+                        scratch, &P.src, &a.src, &P.rcv, &a.rcv, &src_rows, &rcv_rows, tm2d ? &src_any : nullptr,
+                        tm2d ? &rcv_any : nullptr);
+    }
     tg.src_rows = src_rows;
     tg.rcv_rows = rcv_rows;
     // rows with a receiver or source of any shot go to the general (frame) kernels
@@ -1761,7 +2056,65 @@ void backward_impl(const BackwardCall<T>& bc) {
           });
         }
       };
-      if (ok) ok = run_loop(cm.nt, -1, ctrl, st, issue);
+      // host-resident histories (use_async_offload): staged into device rings ahead of use
+      HistRing hr;
+      const ThreadOptions saved_opt = g_opt;
+      const bool off_e = want_model && is_host_memory(bc.E_saved);
+      const bool off_r = want_model && !e_only && is_host_memory(bc.R_saved);
+      if (ok && (off_e || off_r)) {
+        if (kind == kFP8) {
+          set_error("backward: FP8 histories stay on the device (no offload)");
+          ok = false;
+        } else {
+          g_opt.use_graph = 0;
+          g_opt.chunk = std::max(g_opt.chunk, 32);
+          ok = hr.setup(scratch, st, off_e ? const_cast<void*>(bc.E_saved) : nullptr,
+                        off_r ? const_cast<void*>(bc.R_saved) : nullptr, cm.S, cm.nt, a.nt_saved, ncomp, a.frame,
+                        hist_elem_bytes(kind), g_opt.chunk, e_only ? 1 : 0);
+        }
+      }
+      const int clen = std::max(1, g_opt.chunk);
+      // stages reverse chunk c (steps from nt-1-c*clen downwards) into buffer c & 1
+      auto stage_chunk = [&](int c) -> bool {
+        const int t = c * clen;
+        if (t >= cm.nt) return true;
+        int s0, s1;
+        hr.bwd_slots(t, std::min(clen, cm.nt - t), s0, s1);
+        const int b = c & 1;
+        if (!hr.move(b, s0, s1, false)) return false;
+        hr.pending[b] = true;
+        return cuda_ok(cudaEventRecord(hr.done[b], hr.copy), "offload event");
+      };
+      if (ok && hr.on) {
+        // the copy stream starts after everything the call enqueued so far
+        ok = cuda_ok(cudaEventRecord(hr.work[0], st), "offload event") &&
+             cuda_ok(cudaStreamWaitEvent(hr.copy, hr.work[0], 0), "offload wait") && stage_chunk(0) && stage_chunk(1);
+      }
+      auto bhook = [&](int t, int K, int phase) -> bool {
+        if (!hr.on) return true;
+        const int c = t / clen, b = c & 1;
+        if (phase == 0) {
+          int s0, s1;
+          hr.bwd_slots(t, K, s0, s1);
+          if (!cuda_ok(cudaStreamWaitEvent(st, hr.done[b], 0), "offload wait")) return false;
+          if (hr.host[0]) a.E_saved = hr.base(0, b, s0);
+          if (hr.host[1]) a.R_saved = hr.base(1, b, s0);
+          a.comp_stride = hr.comp_stride();
+          return true;
+        }
+        // buffer b is free once the work stream passes this point: stage chunk c + 2 into it
+        return cuda_ok(cudaEventRecord(hr.work[b], st), "offload event") &&
+               cuda_ok(cudaStreamWaitEvent(hr.copy, hr.work[b], 0), "offload wait") && stage_chunk(c + 2);
+      };
+      if (ok) ok = run_loop(cm.nt, -1, ctrl, st, issue, bhook);
+      if (hr.on) {
+        for (int b = 0; b < 2; ++b)
+          if (hr.pending[b]) cudaStreamWaitEvent(st, hr.done[b], 0);
+        a.E_saved = bc.E_saved;
+        a.R_saved = bc.R_saved;
+        a.comp_stride = (long long)a.nt_saved * a.frame;
+      }
+      g_opt = saved_opt;
       if (ok && !tm2d) ok = k3_unpack(g, kg, st, kb, bc.lEx, bc.lEy, bc.lEz, bc.lHx, bc.lHy, bc.lHz);
       if (ok && tm2d) {
         k_unpack2d_pitch<T><<<2048, 256, 0, st>>>(tl.Ez, bc.lEz, (long long)g.nshot * g.NX, g.NY, tg.NYP);
@@ -2062,6 +2415,20 @@ DGB_API int dgb_set_stream(void* stream) {
 DGB_API void dgb_clear_stream(void) {
   g_opt.user_stream = nullptr;
   g_opt.user_stream_set = false;
+}
+
+// Launch-shape choices for the calling thread's next solves (the autotuner's
+// knobs): 2D interior row chunks and frame rows per warp chunk, 3D x chunks,
+// 3D forward kernel family (1 staged, 0 z-streamed, -1 the environment's
+// choice).  Zeros (and -1) restore the built-in heuristics.  Results do not
+// depend on these choices.  Returns 0, or -1 for out-of-range values.
+DGB_API int dgb_set_tuning(int tm_chunks, int tm_frame_rows, int k3_xchunks, int tma) {
+  if (tm_chunks < 0 || tm_frame_rows < 0 || tm_frame_rows > 64 || k3_xchunks < 0 || tma < -1 || tma > 1) return -1;
+  g_opt.tm_chunks = tm_chunks;
+  g_opt.tm_frame_rows = tm_frame_rows;
+  g_opt.k3_xchunks = k3_xchunks;
+  g_opt.tma = tma;
+  return 0;
 }
 
 DGB_API int dgb_set_options(int acc64, int chunk_steps, int use_graph, int fdtd_order) {

@@ -101,6 +101,7 @@ SCALAR_SYMBOLS: Dict[str, Tuple[Tuple[str, ...], Optional[str]]] = {
     "dgb_set_stream": (("void*",), "int"),
     "dgb_clear_stream": ((), None),
     "dgb_set_options": (("int", "int", "int", "int"), "int"),
+    "dgb_set_tuning": (("int", "int", "int", "int"), "int"),
     "dgb_history_bytes": (("int", "int", "int", "int", "long long", "int", "int", "int", "int"), "long long"),
     "dgb_check_fixed_division": (("float", "void*", "void*"), "int"),
     "dgb_set_scratch_retention": (("long long",), "int"),
@@ -271,17 +272,26 @@ def last_error(lib: ctypes.CDLL) -> str:
     return msg.decode("utf-8", "replace") if msg else ""
 
 
+# Launch-shape choices of dgb_set_tuning: the built-in heuristics
+DEFAULT_TUNING = (0, 0, 0, -1)
+
+
 def invoke(name: str, args: Mapping[str, Any], *, fdtd_order: int, stream: Any = None,
-           acc64: bool = True, chunk: int = 16, use_graph: bool = True) -> None:
+           acc64: bool = True, chunk: int = 16, use_graph: bool = True,
+           tuning: Sequence[int] = DEFAULT_TUNING) -> None:
     """Call ``forward``/``backward`` (or their FP64 twins) on ``stream``.
 
-    Raises :class:`NativeLibraryError` with the library's message on failure.
+    ``tuning`` is ``(tm_chunks, tm_frame_rows, k3_xchunks, tma)`` of
+    ``dgb_set_tuning`` (see ``deepgpr_b200.autotune``).  Raises
+    :class:`NativeLibraryError` with the library's message on failure.
     """
     lib = load_library()
     sig, _ = SOLVER_SYMBOLS[name]
     positional = marshal(sig, args)
     if lib.dgb_set_options(int(acc64), int(chunk), int(use_graph), int(fdtd_order)) != 0:
         raise NativeLibraryError("invalid launch options")
+    if lib.dgb_set_tuning(*(int(v) for v in tuning)) != 0:
+        raise NativeLibraryError(f"invalid tuning {tuple(tuning)}")
     handle = 0
     if stream is not None:
         handle = int(getattr(stream, "cuda_stream", stream))

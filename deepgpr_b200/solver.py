@@ -19,6 +19,7 @@ from __future__ import annotations
 
 import math
 import warnings
+import dataclasses
 from dataclasses import dataclass
 from datetime import datetime
 from typing import Any, Dict, Optional, Sequence, Tuple
@@ -91,6 +92,8 @@ class SolverConfig:
     region: str
     acc64: bool = True
     tm2d: bool = False
+    chunk: int = 16                                     # time steps per captured graph
+    tuning: Tuple[int, int, int, int] = (0, 0, 0, -1)   # dgb_set_tuning (see deepgpr_b200.autotune)
 
     @property
     def field_shape(self) -> Tuple[int, int, int]:
@@ -223,7 +226,7 @@ class FDTDFunction(torch.autograd.Function):
         waveform = source_amplitudes.detach().contiguous()
         args = forward_arguments(cfg, tensors, states, e_saved, r_saved, receivers, waveform, storage_type, save_model)
         native.invoke(cfg.entry[0], args, fdtd_order=cfg.fdtd_order, stream=torch.cuda.current_stream(dev),
-                      acc64=cfg.acc64)
+                      acc64=cfg.acc64, chunk=cfg.chunk, tuning=cfg.tuning)
         if cfg.debug:
             _check_finite("forward", receivers=receivers, **dict(zip(STATE_NAMES, states)))
         ctx.cfg = cfg
@@ -263,7 +266,7 @@ class FDTDFunction(torch.autograd.Function):
         args = backward_arguments(cfg, ctx.tensors, lambdas, e_saved, r_saved, data_grad, grad_src, grad_eps,
                                   grad_sig, ctx.want, ctx.storage_type)
         native.invoke(cfg.entry[1], args, fdtd_order=cfg.fdtd_order, stream=torch.cuda.current_stream(dev),
-                      acc64=cfg.acc64)
+                      acc64=cfg.acc64, chunk=cfg.chunk, tuning=cfg.tuning)
         ctx.histories = None
         if cfg.tm2d:
             # Ex, Ey, Hz and their CPML arrays never couple back on the 2D TM path
@@ -507,6 +510,7 @@ def compute(
     gradient_accumulation="float64",
     checkpoint_segments=None,
     checkpoint_shot_batch=None,
+    autotune=False,
 ):
     """2D/3D Maxwell FDTD forward modelling with an exact discrete adjoint on B200.
 
@@ -523,13 +527,23 @@ def compute(
     not fit 80 % of the free device memory, with the longest segments that do.
     ``checkpoint_shot_batch`` fixes the shots per backward batch.  A
     checkpointed solve returns an empty ``E_saved`` (no full history exists).
+
+    ``autotune=True`` picks the launch shapes of the solve with
+    ``deepgpr_b200.autotune`` (short probe solves the first time a problem
+    signature is seen, a kept choice afterwards); results do not change.
     """
     args = dict(locals())
     segments = args.pop("checkpoint_segments")
     shot_batch = args.pop("checkpoint_shot_batch")
+    tune = args.pop("autotune")
     output_directory = normalize_forward_wavefield_directory(save_forward_wavefield_path)
     run_time = datetime.now() if output_directory is not None else None
     cfg, tensors, prepared, states_in = _prepare_solve(**args)
+    if tune:
+        from .autotune import default_tuner, tuning_tuple
+
+        choice = default_tuner().choose(cfg, tensors, states_in, prepared.source_amplitudes)
+        cfg = dataclasses.replace(cfg, chunk=int(choice["chunk"]), tuning=tuning_tuple(choice))
     plan = _checkpoint_plan(cfg, prepared, states_in, segments, shot_batch)
     if plan is not None:
         if output_directory is not None:

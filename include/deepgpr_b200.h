@@ -194,6 +194,14 @@ int dgb_check_fixed_division(float divisor, unsigned long long* mismatches, unsi
  * device.  Returns 0, or -1 with deepgpr_last_error() set. */
 int dgb_set_scratch_retention(long long bytes);
 
+/* No counterpart in the reference.  Launch-shape choices for the calling
+ * thread's next solves (set by deepgpr_b200.autotune): 2D interior row
+ * chunks, 2D frame rows per warp chunk, 3D x chunks, 3D forward kernel family
+ * (1 TMA-staged, 0 z-streamed, -1 the DEEPGPR_B200_TMA environment choice).
+ * 0 / -1 restore the built-in heuristics; results do not depend on them.
+ * Returns 0, or -1 for out-of-range values. */
+int dgb_set_tuning(int tm_chunks, int tm_frame_rows, int k3_xchunks, int tma);
+
 /* No counterpart in the reference (diagnostic).  Bytes in use in the current
  * device's default stream-ordered memory pool (the pool cudaMallocAsync draws
  * on) and its high-water mark; reset_high != 0 first resets the mark to the

@@ -203,3 +203,33 @@ def test_checkpoint_plan_prefers_all_shots_then_the_longest_segments():
     assert p3.segment_steps % 3 == 0 or p3.segment_steps == c3.nt
     with pytest.raises(MemoryError):
         plan_segments(cfg, state, 1000)
+
+
+def test_autotune_coordinate_search_and_cache(tmp_path):
+    from deepgpr_b200 import autotune
+
+    space = [("tm_chunks", (0, 1, 2, 4)), ("tm_frame_rows", (0, 4, 16)), ("chunk", (16, 32))]
+    calls = []
+
+    def cost(c):
+        calls.append(dict(c))
+        return abs(c["tm_chunks"] - 2) + abs(c["tm_frame_rows"] - 4) * 0.1 + (0.5 if c["chunk"] == 16 else 0.0)
+
+    best, seen = autotune.coordinate_search(space, cost)
+    assert (best["tm_chunks"], best["tm_frame_rows"], best["chunk"]) == (2, 4, 32)
+    assert len(calls) == len(seen)            # every candidate measured once
+    assert autotune.tuning_tuple(best) == (2, 4, 0, -1)
+
+    class Cfg:
+        tm2d, nx, ny, nz, pml, nstep, fdtd_order, mode = True, 10, 20, 1, (2, 2, 2, 2, 0, 0), 3, 4, 2
+        dtype = torch.float32
+
+        class storage:
+            kind = 0
+
+    tuner = autotune.Autotuner(tmp_path / "t.json")
+    assert tuner.lookup(Cfg) is None
+    tuner.store(Cfg, best)
+    again = autotune.Autotuner(tmp_path / "t.json")   # read back from the file
+    assert again.lookup(Cfg) == best
+    assert "tm2d|10x20x1" in autotune.signature(Cfg)
