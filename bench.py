@@ -26,7 +26,7 @@ cell-update.
 "serving" (also in the line; ``--only-serving`` prints it alone): a seeded
 Poisson stream with config 4's request mix (nt scaled by 0.1, 40 requests,
 all arriving within ~0.6 s so both paths run at capacity) served by
-``deepgpr_b200.serving.SolveServer`` (8 slots, FP8 histories) and, for
+``deepgpr_b200.serving.SolveServer`` (8 slots, INT8 histories) and, for
 comparison, by plain per-request ``compute`` (+ ``backward``) calls one after
 another (FP32 histories); solves/s and p50/p99 latency of both.
 
@@ -467,7 +467,7 @@ def config3_measure(dev, nt=2500, steps=1):
 
 
 def serving_measure(dev, n=40, slots=8):
-    """Config-4 stream: continuous-batching server (FP8) vs plain per-request launches (FP32)."""
+    """Config-4 stream: continuous-batching server (INT8 histories) vs plain per-request launches (FP32)."""
     from deepgpr_b200.serving import SolveServer, percentile, run_plain
     from deepgpr_b200.synthetic import serving_stream
 
@@ -477,7 +477,7 @@ def serving_measure(dev, n=40, slots=8):
     torch.cuda.synchronize()
     plain = run_plain(reqs, dev, arrivals=arrivals, history="fp32")
     torch.cuda.synchronize()
-    with SolveServer(dev, slots=slots, history="fp8") as srv:
+    with SolveServer(dev, slots=slots, history="int8") as srv:
         for f in [srv.submit(r) for r in warm]:
             f.result()
         t0 = time.perf_counter()
@@ -504,7 +504,7 @@ def serving_measure(dev, n=40, slots=8):
         "sample": f"{n} requests ({kinds['forward']} forward, {kinds['gradient']} gradient), nt scaled by 0.1, "
                   f"arrivals within {arrivals[-1]:.2f} s",
         "plain": dict(sp, history="fp32", path="compute (+ backward) per request, one after another"),
-        "served": dict(ss, history="fp8", slots=slots, peak_running=peak_running,
+        "served": dict(ss, history="int8", slots=slots, peak_running=peak_running,
                        peak_reserved_gib=round(peak_reserved / 2**30, 2)),
         "speedup_solves_per_s": ss["solves_per_s"] / sp["solves_per_s"],
     }

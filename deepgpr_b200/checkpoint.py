@@ -60,7 +60,7 @@ def state_bytes_per_shot(states: Sequence[torch.Tensor], nshot: int) -> int:
 def history_bytes_per_step(cfg, nshot: int = 1) -> int:
     """Device bytes of the history of one saved step of ``nshot`` shots (E, and R unless rebuilt from E)."""
     shape = saved_history_shape(cfg.mode, 1, nshot, *cfg.history_cells)
-    if cfg.storage.compression == "fp8":
+    if cfg.storage.compression in ("fp8", "int8"):
         ncomp = shape[0] if len(shape) == 6 else 1
         per = fp8_history_bytes(ncomp, 1, nshot, math.prod(shape[-3:]), cfg.field_shape, cfg.tm2d)
     else:
@@ -74,18 +74,20 @@ def plan_segments(cfg, state_bytes: int, budget_bytes: int, segment_steps: Optio
 
     Peak memory of a batch of B shots with segments of S steps: the
     checkpoints (B states per segment), one segment's history, and about
-    three more states per shot (the live fields, the adjoint states and the
-    solver's working copies).  S is a multiple of the history sampling
-    interval, so every segment saves the same steps the single call would.
+    four more states per shot of the batch (the live fields, the adjoint
+    states and the solver's working copies), on top of the states and
+    adjoint states of all shots and the gradient accumulators.  S is a
+    multiple of the history sampling interval, so every segment saves the
+    same steps the single call would.
     """
     nt, nshot, interval = cfg.nt, cfg.nstep, cfg.interval
     hist = history_bytes_per_step(cfg)
-    grad_fixed = 3 * 8 * cfg.nx * cfg.ny * cfg.nz
+    fixed = 3 * nshot * state_bytes + 4 * 8 * cfg.nx * cfg.ny * cfg.nz
 
     def peak(b: int, s: int) -> int:
         nseg = -(-nt // s)
         saved = -(-s // interval) + 1
-        return b * (state_bytes * (nseg + 3) + hist * saved) + grad_fixed
+        return b * (state_bytes * (nseg + 4) + hist * saved) + fixed
 
     batches = [shot_batch] if shot_batch else sorted({max(1, nshot // d) for d in range(1, nshot + 1)}, reverse=True)
     for b in batches:
@@ -101,6 +103,12 @@ def plan_segments(cfg, state_bytes: int, budget_bytes: int, segment_steps: Optio
                 return SegmentPlan(b, s, nseg, peak(b, s), 2 if b >= nshot else 3)
     raise MemoryError(f"no checkpoint plan fits {budget_bytes / 2**30:.1f} GiB: one shot with one-step segments "
                       f"needs {peak(1, interval) / 2**30:.1f} GiB")
+
+
+def allocate_history_bytes(config, shape, field_shape, tm2d) -> int:
+    """Bytes of a one-byte history of ``shape`` (payload and tile scales)."""
+    ncomp = shape[0] if len(shape) == 6 else 1
+    return fp8_history_bytes(ncomp, shape[-5], shape[-4], math.prod(shape[-3:]), field_shape, tm2d)
 
 
 def _slice_states(states: Sequence[torch.Tensor], b0: int, b1: int) -> List[torch.Tensor]:
@@ -206,6 +214,22 @@ class CheckpointedFDTDFunction(torch.autograd.Function):
                                   chunk=cfg.chunk, tuning=cfg.tuning)
                 del cur
             lam = [t[b0:b1].clone() if t.numel() else t for t in lambdas] if plan.shot_batch < cfg.nstep else lambdas
+            # one E and one R buffer of the longest segment, reused by every segment of the batch (views of
+            # their leading bytes): fresh buffers per segment would fragment the allocator's cache
+            e_buf = r_buf = None
+            if save_model:
+                nts_max = -(-plan.segment_steps // cfg.interval)
+                shape = saved_history_shape(cfg.mode, nts_max, nb, *cfg.history_cells)
+                e_buf = allocate_history(cfg.storage, shape, cfg.field_shape, cfg.tm2d, dev, False).reshape(-1)
+                rshape = saved_history_shape(cfg.mode, 1, nb, *cfg.history_cells) if rhs_from_e else shape
+                r_buf = allocate_history(cfg.storage, rshape, cfg.field_shape, cfg.tm2d, dev, False).reshape(-1)
+
+            def history_view(buf, shape):
+                if cfg.storage.compression in ("fp8", "int8"):
+                    n = allocate_history_bytes(cfg.storage, shape, cfg.field_shape, cfg.tm2d)
+                    return buf[:n]
+                return buf[:math.prod(shape)].view(shape)
+
             for k in range(len(bounds) - 1, -1, -1):
                 t0, t1 = bounds[k]
                 seg = dataclasses.replace(cfg, nt=t1 - t0, nstep=nb)
@@ -215,9 +239,9 @@ class CheckpointedFDTDFunction(torch.autograd.Function):
                 if save_model:
                     nts = -(-(t1 - t0) // cfg.interval)
                     shape = saved_history_shape(cfg.mode, nts, nb, *cfg.history_cells)
-                    e_saved = allocate_history(cfg.storage, shape, cfg.field_shape, cfg.tm2d, dev, False)
+                    e_saved = history_view(e_buf, shape)
                     rshape = saved_history_shape(cfg.mode, 1, nb, *cfg.history_cells) if rhs_from_e else shape
-                    r_saved = allocate_history(cfg.storage, rshape, cfg.field_shape, cfg.tm2d, dev, False)
+                    r_saved = history_view(r_buf, rshape)
                 rx = torch.empty((nb, t1 - t0, cfg.nrx), device=dev, dtype=dtype)
                 ws = wave[:, t0:t1].contiguous()
                 fargs = forward_arguments(seg, bt, cur, e_saved, r_saved, rx, ws, st_hist if save_model else st_none,
@@ -231,9 +255,10 @@ class CheckpointedFDTDFunction(torch.autograd.Function):
                                            st_hist if save_model else st_none)
                 native.invoke(cfg.entry[1], bargs, fdtd_order=cfg.fdtd_order, stream=stream, acc64=cfg.acc64,
                               chunk=cfg.chunk, tuning=cfg.tuning)
-                del e_saved, r_saved
+                del e_saved, r_saved, fargs, bargs
                 if want_src:
                     grad_src.view(grad_src.shape[0], -1)[:, t0:t1] += gsrc
+            del e_buf, r_buf
             if lam is not lambdas:
                 for full, part in zip(lambdas, lam):
                     if full.numel():

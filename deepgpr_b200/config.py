@@ -34,7 +34,7 @@ CPML_FACES = ("x0", "xm", "y0", "ym", "z0", "zm")
 STORAGE_FLOAT32 = 0
 STORAGE_FLOAT16 = 1
 STORAGE_BFLOAT16 = 2
-STORAGE_INT8 = 3          # reference-only block-INT8 format (not provided here)
+STORAGE_INT8 = 3          # INT8 codes with one FP32 scale per 32-cell tile (this library's layout)
 STORAGE_FP8_E4M3 = 4      # FP8 E4M3 with one FP32 scale per 256-cell tile
 STORAGE_FLOAT64 = 5       # exact histories of the FP64 runs
 STORAGE_KIND_MASK = 0x0F

@@ -227,6 +227,7 @@ __device__ __forceinline__ void with_hist_kind(int kind, F f) {
     case kF16: f(std::integral_constant<int, kF16>()); break;
     case kBF16: f(std::integral_constant<int, kBF16>()); break;
     case kFP8: f(std::integral_constant<int, kFP8>()); break;
+    case kI8: f(std::integral_constant<int, kI8>()); break;
     case kF64: f(std::integral_constant<int, kF64>()); break;
     default: f(std::integral_constant<int, kF32>()); break;
   }
@@ -504,12 +505,12 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_min_blocks<T, R>()) k3v_fwd_
 #pragma unroll
           for (int e = 0; e < 2; ++e) v[e] = fc == 0 ? ex[e] : (fc == 1 ? qEy[R - 1][e] : qEz[R - 1][e]);
           float inv = 1.0f;
-          if (KIND == kFP8) {
+          if (is_tiled(KIND)) {
             float am = 0.0f;
 #pragma unroll
             for (int e = 0; e < 2; ++e)
               if (ib[e]) am = fmaxf(am, fabsf(float(v[e])));
-            const float sc = fp8_scale_of(half_absmax(am));
+            const float sc = tile_scale_of(KIND, half_absmax(am));
             inv = 1.0f / sc;
             if ((lane & 15) == 0 && kk < NZ)
               a.e_scales[(((long long)q * a.nt_saved + slot) * g.nshot + s) * a.ntiles + fp8_tile3(g, i, j, kk)] = sc;
@@ -1039,8 +1040,8 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_min_blocks<T, R>()) k3v_fwd_
             }
           }
           float inv = 1.0f;
-          if (KIND == kFP8) {
-            const float sc = fp8_scale_of(half_absmax(am));
+          if (is_tiled(KIND)) {
+            const float sc = tile_scale_of(KIND, half_absmax(am));
             inv = 1.0f / sc;
             if ((lane & 15) == 0 && kk < NZ)
               a.r_scales[(((long long)q * a.nt_saved + slot) * g.nshot + s) * a.ntiles + fp8_tile3(g, i, j, kk)] = sc;

@@ -1072,7 +1072,7 @@ __global__ void __launch_bounds__(kImage3Threads) k3_image(AdjArgs<T> a, const T
   };
   auto load1 = [&](int sh, int q, T& l, T& e, T& n) {
     float esc = 1.0f, rsc = 1.0f;
-    if (KIND == kFP8) {
+    if (is_tiled(KIND)) {
       const long long si = (((long long)q * a.nt_saved + slot) * nshot + sh) * a.ntiles + tile;
       esc = a.e_scales[si];
       if (!EONLY) rsc = a.r_scales[si];

@@ -458,12 +458,12 @@ __global__ void __launch_bounds__(KT_THREADS, kt_min_blocks<R>())
 #pragma unroll
             for (int e = 0; e < 2; ++e) v[e] = fc == 0 ? zx.at(e, 0) : (fc == 1 ? zy.at(e, 0) : (e == 0 ? yz[-LO].x : yz[-LO].y));
             float inv = 1.0f;
-            if (KIND == kFP8) {
+            if (is_tiled(KIND)) {
               float am = 0.0f;
 #pragma unroll
               for (int e = 0; e < 2; ++e)
                 if (ib[e]) am = fmaxf(am, fabsf(v[e]));
-              const float sc = fp8_scale_of(half_absmax(am));
+              const float sc = tile_scale_of(KIND, half_absmax(am));
               inv = 1.0f / sc;
               if ((lane & 15) == 0 && kc[0] < NZ)
                 a.e_scales[(((long long)q * a.nt_saved + hslot) * g.nshot + s) * a.ntiles + fp8_tile3(g, i, j, kc[0])] =
@@ -709,8 +709,8 @@ __global__ void __launch_bounds__(KT_THREADS, kt_min_blocks<R>())
               }
             }
             float inv = 1.0f;
-            if (KIND == kFP8) {
-              const float sc = fp8_scale_of(half_absmax(am));
+            if (is_tiled(KIND)) {
+              const float sc = tile_scale_of(KIND, half_absmax(am));
               inv = 1.0f / sc;
               if ((lane & 15) == 0 && kc[0] < NZ)
                 a.r_scales[(((long long)q * a.nt_saved + hslot) * g.nshot + s) * a.ntiles + fp8_tile3(g, i, j, kc[0])] =

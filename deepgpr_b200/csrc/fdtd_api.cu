@@ -621,6 +621,7 @@ void launch_tm_image(int kind, bool e_only, bool acc64, cudaStream_t st, const A
     if (kind == kF16) launch_tm_image_k<T, kF16>(e_only, acc64, st, a, lam, tg);
     else if (kind == kBF16) launch_tm_image_k<T, kBF16>(e_only, acc64, st, a, lam, tg);
     else if (kind == kFP8) launch_tm_image_k<T, kFP8>(e_only, acc64, st, a, lam, tg);
+    else if (kind == kI8) launch_tm_image_k<T, kI8>(e_only, acc64, st, a, lam, tg);
     else launch_tm_image_k<T, kF32>(e_only, acc64, st, a, lam, tg);
   }
 }
@@ -654,6 +655,7 @@ void launch_k3_image(int kind, bool e_only, bool acc64, int mode, cudaStream_t s
     if (kind == kF16) by_nc(std::integral_constant<int, kF16>());
     else if (kind == kBF16) by_nc(std::integral_constant<int, kBF16>());
     else if (kind == kFP8) by_nc(std::integral_constant<int, kFP8>());
+    else if (kind == kI8) by_nc(std::integral_constant<int, kI8>());
     else by_nc(std::integral_constant<int, kF32>());
   }
 }
@@ -1338,12 +1340,12 @@ void forward_impl(const ForwardCall<T>& fc) {
     set_error("forward: E-only wavefield history requires sampling interval 1");
     return;
   }
-  if (history && kind != kF32 && kind != kF16 && kind != kBF16 && kind != kFP8 && kind != kF64) {
+  if (history && kind != kF32 && kind != kF16 && kind != kBF16 && !is_tiled(kind) && kind != kF64) {
     set_error("forward: unsupported history storage kind %d", kind);
     return;
   }
-  if (history && kind == kFP8 && e_only) {
-    set_error("forward: FP8 histories keep E and R (E-only reconstruction is not supported for FP8)");
+  if (history && is_tiled(kind) && e_only) {
+    set_error("forward: one-byte (FP8 / INT8) histories keep E and R (no E-only reconstruction)");
     return;
   }
   if (history && (kind == kF64) != (sizeof(T) == 8)) {
@@ -1409,7 +1411,7 @@ void forward_impl(const ForwardCall<T>& fc) {
     a.R_saved = fc.R_saved;
     a.ntiles = (int)fp8_tiles(g, tm2d);
     const int ncomp = cm.mode == 3 ? 3 : 1;
-    if (history && kind == kFP8) {
+    if (history && is_tiled(kind)) {
       const long long vals = (long long)ncomp * a.comp_stride;
       a.e_scales = reinterpret_cast<float*>(static_cast<char*>(fc.E_saved) + fp8_payload_bytes(vals));
       if (keep_r) a.r_scales = reinterpret_cast<float*>(static_cast<char*>(fc.R_saved) + fp8_payload_bytes(vals));
@@ -1593,8 +1595,8 @@ void forward_impl(const ForwardCall<T>& fc) {
       const bool off_e = history && is_host_memory(fc.E_saved);
       const bool off_r = keep_r && is_host_memory(fc.R_saved);
       if (ok && (off_e || off_r)) {
-        if (kind == kFP8) {
-          set_error("forward: FP8 histories stay on the device (no offload)");
+        if (is_tiled(kind)) {
+          set_error("forward: one-byte (FP8 / INT8) histories stay on the device (no offload)");
           ok = false;
         } else {
           g_opt.use_graph = 0;   // the ring base changes from chunk to chunk
@@ -1741,8 +1743,8 @@ void backward_impl(const BackwardCall<T>& bc) {
     set_error("backward: E-only wavefield history requires sampling interval 1");
     return;
   }
-  if (want_model && kind == kFP8 && e_only) {
-    set_error("backward: FP8 histories keep E and R (E-only reconstruction is not supported for FP8)");
+  if (want_model && is_tiled(kind) && e_only) {
+    set_error("backward: one-byte (FP8 / INT8) histories keep E and R (no E-only reconstruction)");
     return;
   }
   if (want_model && (kind == kF64) != (sizeof(T) == 8)) {
@@ -1821,7 +1823,7 @@ void backward_impl(const BackwardCall<T>& bc) {
     a.R_saved = bc.R_saved;
     a.ntiles = (int)fp8_tiles(g, tm2d);
     const int ncomp = cm.mode == 3 ? 3 : 1;
-    if (want_model && kind == kFP8) {
+    if (want_model && is_tiled(kind)) {
       const long long vals = (long long)ncomp * a.comp_stride;
       a.e_scales = reinterpret_cast<const float*>(static_cast<const char*>(bc.E_saved) + fp8_payload_bytes(vals));
       a.r_scales = reinterpret_cast<const float*>(static_cast<const char*>(bc.R_saved) + fp8_payload_bytes(vals));
@@ -2062,8 +2064,8 @@ void backward_impl(const BackwardCall<T>& bc) {
       const bool off_e = want_model && is_host_memory(bc.E_saved);
       const bool off_r = want_model && !e_only && is_host_memory(bc.R_saved);
       if (ok && (off_e || off_r)) {
-        if (kind == kFP8) {
-          set_error("backward: FP8 histories stay on the device (no offload)");
+        if (is_tiled(kind)) {
+          set_error("backward: one-byte (FP8 / INT8) histories stay on the device (no offload)");
           ok = false;
         } else {
           g_opt.use_graph = 0;
@@ -2444,7 +2446,7 @@ DGB_API int dgb_set_options(int acc64, int chunk_steps, int use_graph, int fdtd_
 DGB_API long long dgb_history_bytes(int kind, int ncomp, int nt_saved, int nshot, long long box_cells,
                                     int NX, int NY, int NZ, int tm2d) {
   const long long vals = (long long)ncomp * nt_saved * nshot * box_cells;
-  if (kind == kFP8) {
+  if (is_tiled(kind)) {
     Grid g;
     g.NX = NX; g.NY = NY; g.NZ = NZ;
     const long long tiles = fp8_tiles(g, tm2d != 0);

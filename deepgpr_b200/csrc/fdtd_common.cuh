@@ -26,7 +26,13 @@ constexpr int kMaxShotGroups = 65535;
 
 // History storage kinds (bits 0-3 of storage_type).  0-2 follow the
 // reference (src/DeepGPR/config/constants.py:128-131); 4 and 5 are added here.
-enum HistKind : int { kF32 = 0, kF16 = 1, kBF16 = 2, kFP8 = 4, kF64 = 5 };
+enum HistKind : int { kF32 = 0, kF16 = 1, kBF16 = 2, kI8 = 3, kFP8 = 4, kF64 = 5 };
+
+// Kinds stored as one byte per value with one FP32 scale per tile: FP8 E4M3
+// (value = code * scale, scale = absmax / 448) and INT8 (value = code * scale,
+// code in [-127, 127] rounded to nearest, scale = absmax / 127: a uniform
+// grid, so a tile's largest values keep 8 bits where E4M3 keeps 4).
+__host__ __device__ constexpr bool is_tiled(int kind) { return kind == kFP8 || kind == kI8; }
 
 // Error bits written into Control::error by device code.
 enum DevError : int { kErrSourceRange = 1, kErrReceiverRange = 2 };
@@ -318,6 +324,10 @@ __device__ __forceinline__ void hist_store(void* base, long long idx, T v, int k
       reinterpret_cast<__nv_fp8_storage_t*>(base)[idx] =
           __nv_cvt_float_to_fp8(float(v) * inv_scale, __NV_SATFINITE, __NV_E4M3);
       break;
+    case kI8:
+      reinterpret_cast<signed char*>(base)[idx] =
+          (signed char)max(-127, min(127, __float2int_rn(float(v) * inv_scale)));
+      break;
     case kF64: reinterpret_cast<double*>(base)[idx] = double(v); break;
     default: reinterpret_cast<float*>(base)[idx] = float(v); break;
   }
@@ -332,13 +342,14 @@ __device__ __forceinline__ T hist_load(const void* base, long long idx, int kind
       __half_raw h = __nv_cvt_fp8_to_halfraw(reinterpret_cast<const __nv_fp8_storage_t*>(base)[idx], __NV_E4M3);
       return T(__half2float(__half(h)) * scale);
     }
+    case kI8: return T(float(reinterpret_cast<const signed char*>(base)[idx]) * scale);
     case kF64: return T(reinterpret_cast<const double*>(base)[idx]);
     default: return T(reinterpret_cast<const float*>(base)[idx]);
   }
 }
 
 __host__ __device__ __forceinline__ int hist_elem_bytes(int kind) {
-  return kind == kF32 ? 4 : (kind == kF64 ? 8 : (kind == kFP8 ? 1 : 2));
+  return kind == kF32 ? 4 : (kind == kF64 ? 8 : (is_tiled(kind) ? 1 : 2));
 }
 
 // Block-wide maximum of non-negative values (all threads must call).
@@ -361,6 +372,10 @@ __device__ __forceinline__ float block_absmax(float v, float* red) {
 // floor keeps 1/scale finite for all-but-zero tiles (values below 448e-30
 // are stored as 0 or subnormal FP8, far below FP32 gradient resolution).
 __device__ __forceinline__ float fp8_scale_of(float absmax) { return fmaxf(absmax / 448.0f, 1e-30f); }
+// Tile scale of a one-byte kind (FP8: absmax / 448; INT8: absmax / 127), same floor.
+__device__ __forceinline__ float tile_scale_of(int kind, float absmax) {
+  return kind == kI8 ? fmaxf(absmax / 127.0f, 1e-30f) : fp8_scale_of(absmax);
+}
 
 // ---------------------------------------------------------------------------
 // Point tables (sources, receivers): unique cells sorted ascending; entries

@@ -149,7 +149,7 @@ __global__ void __launch_bounds__(256) k_image(AdjArgs<T> a, const T* lam_x, con
       const bool du = fc == 0 ? dex : (fc == 1 ? dey : dez);
       const long long hix = q * a.comp_stride + slot * a.frame + s * bc + hidx;
       float esc = 1.0f, rsc = 1.0f;
-      if (a.kind == kFP8) {
+      if (is_tiled(a.kind)) {
         const long long si = (((long long)q * a.nt_saved + slot) * g.nshot + s) * a.ntiles + tile;
         esc = a.e_scales[si];
         if (!a.e_only) rsc = a.r_scales[si];

@@ -181,9 +181,9 @@ __device__ __forceinline__ void tm_fwd_h_body(const TiledFwd<T>& P, const TmBuf<
       long long hk = 0;
       const bool ib = cv && in_box(a.box, i, j, 0, hk);
       float inv = 1.0f;
-      if (a.kind == kFP8) {
+      if (is_tiled(a.kind)) {
         // one scale per warp strip row: tile i * nseg + seg
-        const float sc = fp8_scale_of(warp_absmax(ib ? fabsf(float(cur)) : 0.0f));
+        const float sc = tile_scale_of(a.kind, warp_absmax(ib ? fabsf(float(cur)) : 0.0f));
         inv = 1.0f / sc;
         if (lane == 0) a.e_scales[((long long)slot * g.nshot + s) * a.ntiles + (long long)i * tg.nseg + wp.seg] = sc;
       }
@@ -387,8 +387,8 @@ __device__ __forceinline__ void tm_fwd_e_body(const TiledFwd<T>& P, const TmBuf<
           rv = cb != T(0) ? (ez - aeff * ez0) / cb : T(0);
         }
         float inv = 1.0f;
-        if (a.kind == kFP8) {
-          const float sc = fp8_scale_of(warp_absmax(inbox ? fabsf(float(rv)) : 0.0f));
+        if (is_tiled(a.kind)) {
+          const float sc = tile_scale_of(a.kind, warp_absmax(inbox ? fabsf(float(rv)) : 0.0f));
           if (lane == 0) a.r_scales[((long long)slot * g.nshot + s) * a.ntiles + (long long)i * tg.nseg + wp.seg] = sc;
           inv = 1.0f / sc;
         }
@@ -798,7 +798,7 @@ __global__ void __launch_bounds__(kImageThreads) tm_image(AdjArgs<T> a, const T*
   };
   auto load1 = [&](long long so, T& l, T& e, T& n) {
     float esc = 1.0f, rsc = 1.0f;
-    if (KIND == kFP8) {
+    if (is_tiled(KIND)) {
       esc = a.e_scales[sc0 + so * a.ntiles];
       if (!EONLY) rsc = a.r_scales[sc0 + so * a.ntiles];
     }
@@ -1009,8 +1009,8 @@ __global__ void __launch_bounds__(32 * TM_WARPS) tmi_fwd_h(TiledFwd<T> P, TmBuf<
         if (ib[e]) am = fmaxf(am, fabsf(float(q[R - 1][e])));
       }
       float inv = 1.0f;
-      if (a.kind == kFP8) {
-        const float sc = fp8_scale_of(tile8_absmax(am));
+      if (is_tiled(a.kind)) {
+        const float sc = tile_scale_of(a.kind, tile8_absmax(am));
         inv = 1.0f / sc;
         if (act && (lane & 7) == 0)
           a.e_scales[((long long)slot * g.nshot + s) * a.ntiles + (long long)i * tg.nseg + wp.seg + (lane >> 3)] = sc;
@@ -1123,8 +1123,8 @@ __global__ void __launch_bounds__(32 * TM_WARPS) tmi_fwd_e(TiledFwd<T> P, TmBuf<
         }
       }
       float inv = 1.0f;
-      if (a.kind == kFP8) {
-        const float sc = fp8_scale_of(tile8_absmax(am));
+      if (is_tiled(a.kind)) {
+        const float sc = tile_scale_of(a.kind, tile8_absmax(am));
         if (act && (lane & 7) == 0)
           a.r_scales[((long long)slot * g.nshot + s) * a.ntiles + (long long)i * tg.nseg + wp.seg + (lane >> 3)] = sc;
         inv = 1.0f / sc;

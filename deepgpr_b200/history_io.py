@@ -73,9 +73,9 @@ def load_forward_wavefield(path: Any) -> torch.Tensor:
     if torch.is_tensor(payload):
         return payload
     wavefield = payload["wavefield"]
-    if payload.get("compression") == "fp8":
+    if payload.get("compression") in ("fp8", "int8"):
         from .storage import decode_fp8_history
 
         return decode_fp8_history(wavefield, payload["uncompressed_shape"], tuple(payload["field_shape"]),
-                                  tuple(payload["history_origin"]), bool(payload["tm2d"]))
+                                  tuple(payload["history_origin"]), bool(payload["tm2d"]), payload["compression"])
     return wavefield

@@ -22,9 +22,10 @@ admitted requests therefore run concurrently on the GPU, and every solve's time
 loop is replayed from CUDA graphs captured per 16-step chunk.  Gradient solves
 call the native forward and adjoint directly from the slot's thread
 (``solver.misfit_gradient``), so they do not queue behind PyTorch's single
-per-device autograd thread.  They keep FP8 E4M3 histories with per-tile scales
-by default (``history="fp8"``), which shrinks each solve's footprint and
-history traffic; ``history="fp32"`` keeps the exact FP32 E-only histories.
+per-device autograd thread.  They keep one-byte INT8 histories with per-tile scales
+by default (``history="int8"``; ``"fp8"`` stores E4M3 codes on the same tiles
+at about four times the gradient error), which shrinks each solve's footprint
+and history traffic; ``history="fp32"`` keeps the exact FP32 E-only histories.
 
 The result of a request does not depend on what else is running: the kernels
 are deterministic and no arithmetic is shared between requests.
@@ -102,15 +103,15 @@ def _field_cells(ext: Sequence[int]) -> int:
     return (ext[0] + 1) * (ext[1] + 1) * (ext[2] + 1)
 
 
-def footprint_bytes(req: SolveRequest, history: str = "fp8") -> int:
+def footprint_bytes(req: SolveRequest, history: str = "int8") -> int:
     """Upper estimate of the device memory a request holds while it runs.
 
     Counts, in FP32 unless stated: the 6 field and 24 CPML state arrays (and
     their adjoint copies for a gradient), 3 padded material and 6 coefficient
     arrays, the solver's working copy of the fields and 5 coefficients (z
     pitch rounded up to 32), receivers (observed data and residual for a
-    gradient), the histories (FP8: E and R, one byte each plus one scale per 32
-    values; FP32: E only, plus the last E^(n+1) frame), the CPML weight
+    gradient), the histories (INT8 / FP8: E and R, one byte each plus one scale
+    per 32 values; FP32: E only, plus the last E^(n+1) frame), the CPML weight
     scratch and the FP64 gradient accumulators, plus 25 % and 64 MiB of
     margin for the allocators' rounding and the point tables.
     """
@@ -134,7 +135,7 @@ def footprint_bytes(req: SolveRequest, history: str = "fp8") -> int:
     if req.kind == "gradient":
         ncomp = 3 if req.mode == 3 else 1
         box = ext[0] * ext[1] * ext[2]
-        if history == "fp8":
+        if history in ("fp8", "int8"):
             frames = 2 * (nt + 1) * ncomp * shots * box
             hist = frames + frames // 32 * 4
         else:
@@ -171,7 +172,7 @@ def _solve(req: SolveRequest, device: torch.device, history: str, stream: torch.
         elif req.kind == "gradient":
             if req.observed is None:
                 raise ValueError("a gradient request needs observed receiver data")
-            comp = "fp8" if history == "fp8" else "none"
+            comp = history if history in ("fp8", "int8") else "none"
             loss, ge, gs, _ = misfit_gradient(device, dev(req.observed), eps_r=dev(req.eps_r),
                                               sigma=dev(req.sigma), wavefield_compression=comp, **kw)
             res.loss = float(loss.cpu())
@@ -194,12 +195,12 @@ class SolveServer:
     """
 
     def __init__(self, device: Any = None, slots: int = 8, memory_budget: Optional[int] = None,
-                 history: str = "fp8", run: Optional[Callable[[SolveRequest, int], SolveResult]] = None,
+                 history: str = "int8", run: Optional[Callable[[SolveRequest, int], SolveResult]] = None,
                  footprint: Optional[Callable[[SolveRequest], int]] = None):
         if slots < 1:
             raise ValueError("slots must be >= 1")
-        if history not in ("fp8", "fp32"):
-            raise ValueError("history must be 'fp8' or 'fp32'")
+        if history not in ("fp8", "int8", "fp32"):
+            raise ValueError("history must be 'fp8', 'int8' or 'fp32'")
         self.history = history
         if device is not None:
             self.device = torch.device(device)
@@ -368,7 +369,7 @@ def run_plain(requests: Sequence[SolveRequest], device: Any, arrivals: Optional[
         else:
             eps = dev(req.eps_r).requires_grad_(True)
             sig = dev(req.sigma).requires_grad_(True)
-            comp = "fp8" if history == "fp8" else "none"
+            comp = history if history in ("fp8", "int8") else "none"
             rx = dg.compute(device, eps_r=eps, sigma=sig, wavefield_compression=comp, **kw)[-1]
             loss = 0.5 * ((rx - dev(req.observed)) ** 2).sum()
             loss.backward()

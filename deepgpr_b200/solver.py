@@ -10,7 +10,8 @@ Contract (src/DeepGPR/solver/modeling.py:261-671, src/DeepGPR/solver/autograd.py
   model's shape (the CPML sensitivities are folded onto the edge cells).
 
 Everything runs in the CUDA library; a CPU device raises.  Two additions:
-``wavefield_compression="fp8"`` (E4M3 histories with per-tile scales) and the
+``wavefield_compression="fp8"`` (E4M3 histories with per-tile scales; ``"int8"``
+gives integer codes on the same tiles) and the
 keyword ``precision=torch.float64`` (the same kernels instantiated in double,
 used as the FP64 reference of the FP32 path).
 """
@@ -395,8 +396,8 @@ def _prepare_solve(
     if isinstance(interval, bool) or not isinstance(interval, int) or interval < 1:
         raise ValueError("model_gradient_sampling_interval must be a positive integer or 'auto'.")
     storage_dtype = normalize_storage_dtype(wavefield_storage_dtype)
-    int8_request = isinstance(wavefield_compression, str) and wavefield_compression.lower() == "int8"
     compression = normalize_compression(wavefield_compression)
+    int8_request = compression == "int8"
     normalize_choice("wavefield_conversion_backend", wavefield_conversion_backend,
                      ("auto", "legacy", "native_scalar", "native_vec2"))
     normalize_choice("int8_reduction_backend", int8_reduction_backend, ("auto", "current", "cub_block", "warp_shuffle"))
@@ -404,12 +405,12 @@ def _prepare_solve(
         raise ValueError("wavefield_compression_rate is only meaningful for the optional ZFP backend.")
     if wavefield_compression_block_size is not None and not int8_request:
         raise ValueError("wavefield_compression_block_size applies to the reference's INT8 format only.")
-    if compression == "fp8" and storage_dtype != torch.float32:
-        raise ValueError("wavefield_storage_dtype must stay float32 with wavefield_compression='fp8'.")
+    if compression in ("fp8", "int8") and storage_dtype != torch.float32:
+        raise ValueError(f"wavefield_storage_dtype must stay float32 with wavefield_compression='{compression}'.")
     if not save_wavefield_history and use_async_offload:
         raise ValueError("use_async_offload=True is incompatible with save_wavefield_history=False.")
-    if use_async_offload and compression == "fp8":
-        raise ValueError("use_async_offload=True is incompatible with device-resident FP8 histories.")
+    if use_async_offload and compression in ("fp8", "int8"):
+        raise ValueError("use_async_offload=True is incompatible with device-resident one-byte (FP8 / INT8) histories.")
     if save_forward_wavefield_path is not None and not save_wavefield_history:
         raise ValueError("save_forward_wavefield_path requires save_wavefield_history=True.")
     rhs_mode = normalize_choice("wavefield_rhs_history", wavefield_rhs_history, ("auto", "stored", "reconstructed"))
@@ -437,8 +438,8 @@ def _prepare_solve(
         raise ValueError("mode=2 is an exact model-gradient mode only for 2D Ez-TM modeling. "
                          "Use mode=3 for 3D or other electric-field components.")
     lossless = compression == "none" and storage_dtype == torch.float32
-    if compression == "fp8" and rhs_mode == "reconstructed":
-        raise ValueError("FP8 histories keep the E and R pair; use wavefield_rhs_history='stored' or 'auto'.")
+    if compression in ("fp8", "int8") and rhs_mode == "reconstructed":
+        raise ValueError("One-byte histories keep the E and R pair; use wavefield_rhs_history='stored' or 'auto'.")
     reconstruct = resolve_rhs_reconstruction(rhs_mode, interval, stores_model,
                                              lossless or precision == torch.float64)
     storage = storage_config(storage_dtype, compression, precision)
@@ -565,8 +566,9 @@ def compute(
         origin, cells = history_box(cfg.nx, cfg.ny, cfg.nz, cfg.pml, cfg.region)
         shape = saved_history_shape(cfg.mode, saved_time_steps(cfg.nt, cfg.interval), cfg.nstep, *cells)
         metadata = None
-        if cfg.storage.compression == "fp8":
-            metadata = {"compression": "fp8", "uncompressed_shape": shape, "field_shape": cfg.field_shape,
+        if cfg.storage.compression in ("fp8", "int8"):
+            metadata = {"compression": cfg.storage.compression, "uncompressed_shape": shape,
+                        "field_shape": cfg.field_shape,
                         "history_origin": origin, "tm2d": cfg.tm2d}
         if cfg.region == "physical":
             metadata = dict(metadata or {})
@@ -598,7 +600,7 @@ def _checkpoint_plan(cfg: SolverConfig, prepared, states, segments, shot_batch):
     from .checkpoint import plan_segments, state_bytes_per_shot
 
     free, _ = torch.cuda.mem_get_info(cfg.device)
-    budget = int(0.8 * free)
+    budget = int(0.7 * free)
     state = state_bytes_per_shot(states, cfg.nstep)
     plan = plan_segments(cfg, state, budget, None if auto else min(segments, cfg.nt), shot_batch)
     if auto and plan.nsegments == 1 and plan.shot_batch >= cfg.nstep:

@@ -6,17 +6,27 @@ History layout (as src/DeepGPR/solver/storage.py:359-369): ``E_saved`` is
 the extended grid or, with ``"physical"``, the physical model only
 (storage.py:161-195).
 
-FP8 histories (``wavefield_compression="fp8"``, kind 4) store one E4M3 byte per
-value followed, after 256-byte alignment, by one FP32 scale per
-(component, saved step, shot, tile): the value is ``fp8 * scale`` with
-``scale = absmax(tile) / 448``.  A tile is the cell block one forward CTA
-writes in one x plane: 32 (z) x 8 (y) cells in 3D, 128 (y) cells on the 2D TM
-path.  FP8 histories always keep the E and R pair.
+One-byte histories keep one byte per value followed, after 256-byte
+alignment, by one FP32 scale per (component, saved step, shot, tile); a tile
+is 32 cells of one row (32 z columns of an (x, y) row in 3D, 32 y columns of
+an x row on the 2D TM path), and they always keep the E and R pair:
+
+* ``wavefield_compression="fp8"`` (kind 4): E4M3 codes, value ``code * scale``
+  with ``scale = absmax(tile) / 448`` -- about 4 significant bits for every
+  value of the tile;
+* ``wavefield_compression="int8"`` (kind 3, the reference's option name):
+  signed integer codes in [-127, 127] rounded to nearest, value
+  ``code * scale`` with ``scale = absmax(tile) / 127`` -- a uniform grid, so the
+  tile's largest values, which dominate the imaging sums, keep 8 bits.  The
+  reference's INT8 history uses its own block shape and packing
+  (src/DeepGPR/solver/storage.py:372-414); this one shares the FP8 layout, so
+  the reference's Python does not hand its INT8 layout to this library
+  (``deepgpr_supports_int8_wavefield`` is 0) while this package's own
+  ``compute`` accepts the option.
 """
 
 from __future__ import annotations
 
-import warnings
 from typing import Any, NamedTuple, Optional, Sequence, Tuple
 
 import torch
@@ -31,6 +41,7 @@ from .config import (
     STORAGE_FLOAT32,
     STORAGE_FLOAT64,
     STORAGE_FP8_E4M3,
+    STORAGE_INT8,
 )
 
 TILE_Z, TILE_Y, TILE_2D = 32, 1, 32
@@ -59,9 +70,6 @@ def normalize_storage_dtype(value: Any) -> torch.dtype:
     return value
 
 
-_INT8_WARNED = False
-
-
 def normalize_compression(value: Any) -> str:
     if value is None:
         return "none"
@@ -71,20 +79,11 @@ def normalize_compression(value: Any) -> str:
     if value not in ("none", "fp8", "int8", "zfp"):
         raise ValueError("wavefield_compression must be 'none', 'fp8', 'int8', or 'zfp'.")
     if value == "zfp":
-        raise NotImplementedError("wavefield_compression='zfp' has no block decoder in this library; use 'fp8'.")
-    if value == "int8":
-        global _INT8_WARNED
-        if not _INT8_WARNED:
-            _INT8_WARNED = True
-            warnings.warn(
-                "wavefield_compression='int8' is served by this library's FP8 history (E4M3 values with one "
-                "FP32 scale per 32-value tile) instead of the reference's block-INT8 layout; gradients carry "
-                "a comparable quantisation error and saved history files hold the FP8 layout.",
-                UserWarning,
-                stacklevel=3,
-            )
-        return "fp8"
+        raise NotImplementedError("wavefield_compression='zfp' has no block decoder in this library; use 'int8'.")
     return value
+
+
+ONE_BYTE = ("fp8", "int8")   # compressions stored as one byte per value plus tile scales
 
 
 def normalize_choice(name: str, value: Any, choices: Sequence[str]) -> str:
@@ -178,6 +177,8 @@ def storage_config(dtype: torch.dtype, compression: str, precision: torch.dtype)
         return StorageConfig(torch.float64, "none", STORAGE_FLOAT64)
     if compression == "fp8":
         return StorageConfig(torch.uint8, "fp8", STORAGE_FP8_E4M3)
+    if compression == "int8":
+        return StorageConfig(torch.uint8, "int8", STORAGE_INT8)
     return StorageConfig(dtype, "none", KIND_OF_DTYPE[dtype])
 
 
@@ -186,7 +187,7 @@ def allocate_history(
     pinned: bool
 ) -> torch.Tensor:
     """One history buffer (``E_saved`` or ``R_saved``) for ``shape``."""
-    if config.compression == "fp8":
+    if config.compression in ONE_BYTE:
         ncomp = shape[0] if len(shape) == 6 else 1
         nt_saved, nstep = shape[-5], shape[-4]
         box = shape[-3] * shape[-2] * shape[-1]
@@ -199,9 +200,9 @@ def allocate_history(
 
 def decode_fp8_history(
     packed: torch.Tensor, shape: Sequence[int], field_shape: Tuple[int, int, int], origin: Tuple[int, int, int],
-    tm2d: bool = False,
+    tm2d: bool = False, compression: str = "fp8",
 ) -> torch.Tensor:
-    """Decode an FP8 history into float32 of ``shape`` (diagnostics; not used by backward).
+    """Decode a one-byte (FP8 or INT8) history into float32 of ``shape`` (diagnostics; not used by backward).
 
     ``field_shape`` is ``(NX, NY, NZ)`` of the field grid and ``origin`` the
     history box origin.
@@ -210,7 +211,8 @@ def decode_fp8_history(
     full = shape if len(shape) == 6 else (1,) + shape
     ncomp, nt_saved, nstep, hx, hy, hz = full
     values = ncomp * nt_saved * nstep * hx * hy * hz
-    payload = packed[:values].view(torch.float8_e4m3fn).to(torch.float32).reshape(full)
+    codes = packed[:values].view(torch.float8_e4m3fn if compression == "fp8" else torch.int8)
+    payload = codes.to(torch.float32).reshape(full)
     tiles = fp8_tiles(field_shape, tm2d)
     offset = (values + 255) // 256 * 256
     scales = packed[offset : offset + ncomp * nt_saved * nstep * tiles * 4].view(torch.float32)

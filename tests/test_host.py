@@ -127,19 +127,44 @@ def test_compute_option_errors_match_reference():
                    eps_r=eps, sigma=sig, save_wavefield_history=False, use_async_offload=True)
 
 
-def test_int8_compression_is_served_by_fp8_with_one_warning(monkeypatch):
-    """Reference callers asking for the block-INT8 history get the FP8 history, warned once."""
+def test_int8_and_fp8_compression_options():
+    """'int8' (the reference's option name) selects this library's INT8 tile history, kind 3."""
     from deepgpr_b200 import storage
 
-    monkeypatch.setattr(storage, "_INT8_WARNED", False)
-    with pytest.warns(UserWarning, match="FP8"):
-        assert storage.normalize_compression("int8") == "fp8"
-    import warnings
-
-    with warnings.catch_warnings():
-        warnings.simplefilter("error")
-        assert storage.normalize_compression("INT8") == "fp8"
+    assert storage.normalize_compression("INT8") == "int8"
     assert storage.normalize_compression("fp8") == "fp8"
+    cfg = storage.storage_config(torch.float32, "int8", torch.float32)
+    assert cfg.kind == 3 and cfg.compression == "int8" and cfg.dtype == torch.uint8
+    shape = (3, 4, 2, 5, 6, 40)
+    buf = storage.allocate_history(cfg, shape, (6, 7, 41), False, "cpu", False)
+    assert buf.numel() == storage.fp8_history_bytes(3, 4, 2, 5 * 6 * 40, (6, 7, 41), False)
+
+
+def test_int8_decoder_rounds_trip_within_half_a_step():
+    """Tile codes round(x / s), s = absmax / 127: decoding is within s / 2 of every value."""
+    from deepgpr_b200 import storage
+
+    g = torch.Generator().manual_seed(4)
+    full = (1, 2, 1, 3, 4, 64)
+    x = torch.randn(full, generator=g)
+    field = (4, 5, 65)
+    tiles = storage.fp8_tiles(field, False)
+    values = x.numel()
+    packed = torch.zeros((values + 255) // 256 * 256 + 2 * tiles * 4, dtype=torch.uint8)
+    tile = storage.fp8_tile_of(torch.arange(3).view(3, 1, 1), torch.arange(4).view(1, 4, 1),
+                               torch.arange(64).view(1, 1, 64), field, False).expand(3, 4, 64).reshape(-1)
+    scales = torch.full((1, 2, 1, tiles), 1e-30)
+    flat = x.reshape(1, 2, 1, -1)
+    for t in range(2):
+        for u in tile.unique().tolist():
+            sel = tile == u
+            scales[0, t, 0, u] = max(float(flat[0, t, 0, sel].abs().max()) / 127.0, 1e-30)
+    s_cell = scales[0, :, 0][:, tile].reshape(full)
+    codes = torch.clamp(torch.round(x / s_cell), -127, 127).to(torch.int8)
+    packed[:values] = codes.reshape(-1).view(torch.uint8)
+    packed[(values + 255) // 256 * 256:] = scales.reshape(-1).view(torch.uint8)
+    out = storage.decode_fp8_history(packed, full, field, (0, 0, 0), False, "int8")
+    assert torch.all((out - x).abs() <= 0.5 * s_cell + 1e-7)
 
 
 def test_checkpoint_initial_field_shapes():
