@@ -115,6 +115,16 @@ def test_history_storage_kinds(kind, rhs, cuda_device, oracle_lib):
     _compare(got, ref)
 
 
+@pytest.mark.parametrize("order", [4, 8])
+@pytest.mark.parametrize("kind", [1, 2])
+def test_3d_stored_rhs_history_kinds(kind, order, cuda_device, oracle_lib):
+    """3D FP16 / BF16 histories with stored R^n (config 3's history mode), orders 4 and 8."""
+    p = problem_3d(nt=40, order=order, pml=3, storage_kind=kind, rhs_from_e=False, want_source=True)
+    ref = driver.run(p, "oracle")
+    got = run_product(p, cuda_device)
+    _compare(got, ref, grads=("grad_eps", "grad_sigma", "grad_source"))
+
+
 def test_sampling_interval(cuda_device, oracle_lib):
     p = problem_2d(nt=101, order=2, interval=4, rhs_from_e=False)
     ref = driver.run(p, "oracle")
