@@ -27,6 +27,7 @@
 #include "fdtd_3d.cuh"
 #include "fdtd_3d_adj.cuh"
 #include "fdtd_3d_fast.cuh"
+#include "fdtd_3d_wide.cuh"
 
 #define DGB_API extern "C" __attribute__((visibility("default")))
 
@@ -55,7 +56,7 @@ struct ThreadOptions {
   int tm_chunks = 0;       // 2D: row chunks of the interior rectangles
   int tm_frame_rows = 0;   // 2D: rows per frame warp chunk
   int k3_xchunks = 0;      // 3D: x chunks of the z-streamed and staged kernels
-  int tma = -1;            // 3D forward: staged (TMA) kernels 1, z-streamed 0, -1 DEEPGPR_B200_TMA
+  int tma = -1;            // 3D FP32 forward family: 0 z-streamed, 1 staged (TMA), 2 wide, -1 automatic
 };
 thread_local ThreadOptions g_opt;
 
@@ -140,11 +141,35 @@ struct StreamSet {
 };
 thread_local std::vector<StreamSet> g_streams;
 
+// Scratch retention of the default memory pool.  With the CUDA default (a
+// release threshold of 0) the pool unmaps a call's freed scratch at the next
+// synchronisation and the next call maps it again; on virtualised hosts those
+// mappings took 90-630 ms at random points of back-to-back solves (the GPU
+// idle meanwhile).  So on first use of a device the library keeps up to
+// min(4 GiB, 1/32 of the device memory) cached, unless the caller has set
+// the retention (dgb_set_scratch_retention).
+constexpr int kMaxDevices = 64;
+std::atomic<bool> g_retention_set[kMaxDevices];
+
+void default_retention(int dev) {
+  if (dev < 0 || dev >= kMaxDevices || g_retention_set[dev].exchange(true)) return;
+  size_t free_b = 0, total_b = 0;
+  cudaMemPool_t pool;
+  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess || cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  unsigned long long keep = std::min<unsigned long long>(4ULL << 30, total_b / 32);
+  cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  cudaGetLastError();
+}
+
 StreamSet* stream_set() {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
   for (auto& s : g_streams)
     if (s.device == dev) return &s;
+  default_retention(dev);
   StreamSet s;
   s.device = dev;
   if (cudaStreamCreateWithFlags(&s.work, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
@@ -682,6 +707,25 @@ int split_launch(cudaStream_t st, const StreamSet* ss, const TmPlan& pl, FrameFn
 
 dim3 tm_grid(const TmGeom& tg) { return dim3((unsigned)std::max<long long>(1, (tg.nwarps + TM_WARPS - 1) / TM_WARPS)); }
 
+bool env_flag(const char* name);
+
+// A 2D half step: the frame and interior kernels as two launches on two
+// streams, or fused into one launch (fused(grid, frame CTAs)) when
+// DEEPGPR_B200_TM_FUSED=1 (measured 0-10 % slower per half step on the
+// 400 x 800 x 32-shot grid).  Returns the number of kernels launched.
+template <typename FusedFn, typename FrameFn, typename InteriorFn>
+int tm_launch(cudaStream_t st, const StreamSet* ss, const TmPlan& pl, FusedFn fused, FrameFn frame,
+              InteriorFn interior) {
+  static const bool fuse = env_flag("DEEPGPR_B200_TM_FUSED");
+  if (pl.interior.nwarps > 0 && fuse) {
+    const unsigned nfb = (unsigned)((pl.frame.nwarps + TM_WARPS - 1) / TM_WARPS);
+    const unsigned nib = (unsigned)((pl.interior.nwarps + TM_WARPS - 1) / TM_WARPS);
+    fused(dim3(nfb + nib), nfb);
+    return 1;
+  }
+  return split_launch(st, ss, pl, frame, interior);
+}
+
 // 3D working copy: z pitch, strips, y tiles and x chunks.  The chunking keeps
 // the last wave of CTAs nearly full (occupancy of the forward H kernel).
 // Calls f(R, EQ, GEN) with compile-time constants (std::integral_constant)
@@ -1194,11 +1238,117 @@ bool env_flag(const char* name) {
   return v && v[0] && v[0] != '0';
 }
 
-// Whether the staged kernels take a 3D FP32 forward solve: selected with
-// DEEPGPR_B200_TMA=1, the single-face CPML form (or none), TMA plane
-// coordinates inside int32, and the driver's tensor-map encoder available.
+// 3D FP32 forward kernel family: the tuning knob when set (0 z-streamed,
+// 1 staged, 2 wide), else DEEPGPR_B200_TMA=1 selects the staged kernels and
+// DEEPGPR_B200_WIDE=1 the wide ones.
+int k3_family() {
+  if (g_opt.tma >= 0) return g_opt.tma;
+  if (env_flag("DEEPGPR_B200_TMA")) return 1;
+  return env_flag("DEEPGPR_B200_WIDE") ? 2 : 0;
+}
+
+// Whether the wide kernels take a 3D FP32 forward solve: radius <= 2, the
+// single-face CPML form (or none) and at most 64 z-face cells of E and of H
+// in every 128-column strip.
+bool k3w_usable(const Grid& g, const int* p, bool has_cpml, int R) {
+  if (R > 2) return false;
+  if (!has_cpml) return true;
+  if (!k3_cpml_single(g, p)) return false;
+  const int zp = (g.NZ + 31) / 32 * 32;
+  for (int k0 = 0; k0 < zp; k0 += KWW)
+    if (zslots<false>(p[4], p[5], g.NZ, k0).n() > 64 || zslots<true>(p[4], p[5], g.NZ, k0).n() > 64) return false;
+  return true;
+}
+
+// x chunks of a streamed 3D launch of `per` CTAs per chunk: the count keeps
+// the last wave nearly full and each chunk long against its halo planes.
+int k3_pick_xchunks(int NX, long long per, double resident, double halo) {
+  int best = 1;
+  double best_eff = -1.0;
+  for (int n = 1; n <= std::max(1, std::min(64, NX / 16)); ++n) {
+    const int xc = (NX + n - 1) / n;
+    const int nch = (NX + xc - 1) / xc;
+    const double nb = (double)per * nch;
+    const double waves = std::ceil(nb / resident);
+    const double eff = nb / (waves * resident) * (double)xc / (xc + halo);
+    if (eff > best_eff + 1e-3) {
+      best_eff = eff;
+      best = n;
+    }
+  }
+  if (g_opt.k3_xchunks > 0) best = std::min(g_opt.k3_xchunks, NX);
+  return best;
+}
+
+// Dynamic shared memory of a wide kernel (its staging ring), granted once.
+// KIND: 0 H half step, 1 E half step, 2 E half step of the pass form.
+template <int R, bool EQ, int KIND>
+bool k3w_prepare() {
+  static const bool ok = [] {
+    auto kernel = KIND == 0 ? (void (*)(TiledFwd<float>, K3Buf<float>, K3WGeom))k3w_fwd_h<R, EQ>
+                            : (KIND == 1 ? k3w_fwd_e<R, EQ, false> : k3w_fwd_e<R, EQ, true>);
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                kw_smem_bytes<R, KIND != 0>()) == cudaSuccess;
+  }();
+  return ok;
+}
+
+template <int R>
+bool k3w_ready_r() {
+  return k3w_prepare<R, true, 0>() && k3w_prepare<R, true, 1>() && k3w_prepare<R, true, 2>() &&
+         k3w_prepare<R, false, 0>() && k3w_prepare<R, false, 1>() && k3w_prepare<R, false, 2>();
+}
+
+// Every instantiation is granted its shared memory before any launch (the
+// launches may be captured into graphs).
+bool k3w_ready() { return k3w_ready_r<1>() && k3w_ready_r<2>(); }
+
+K3WGeom k3w_layout(const Grid& g, int zp) {
+  K3WGeom kg;
+  memset(&kg, 0, sizeof(kg));
+  kg.zp = zp;
+  kg.nzs = (zp + KWW - 1) / KWW;
+  kg.nyt = (g.NY + KW_WARPS - 1) / KW_WARPS;
+  int blocks = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k3w_fwd_e<2, true, false>, 32 * KW_WARPS,
+                                                    kw_smem_bytes<2, true>()) != cudaSuccess ||
+      blocks < 1) {
+    cudaGetLastError();
+    blocks = KW_MIN_BLOCKS;
+  }
+  const long long per = (long long)g.nshot * kg.nzs * kg.nyt;
+  const int n = k3_pick_xchunks(g.NX, per, (double)sm_count() * blocks, 3.0);
+  kg.xc = (g.NX + n - 1) / n;
+  kg.nchunk = (g.NX + kg.xc - 1) / kg.xc;
+  kg.nblocks = per * kg.nchunk;
+  return kg;
+}
+
+// KIND: 0 H half step, 1 E half step, 2 E half step of the pass form
+template <int KIND>
+void k3w_launch(int R, bool eq, cudaStream_t st, const TiledFwd<float>& P, const K3Buf<float>& kf,
+                const K3WGeom& kg) {
+  const dim3 grid((unsigned)kg.nblocks), block(32, KW_WARPS);
+  auto go = [&](auto RR, auto E) {
+    constexpr int RV = decltype(RR)::value;
+    constexpr bool EV = decltype(E)::value;
+    constexpr int bytes = kw_smem_bytes<RV, KIND != 0>();
+    if constexpr (KIND == 0) k3w_fwd_h<RV, EV><<<grid, block, bytes, st>>>(P, kf, kg);
+    else k3w_fwd_e<RV, EV, KIND == 2><<<grid, block, bytes, st>>>(P, kf, kg);
+  };
+  if (R == 1) {
+    if (eq) go(std::integral_constant<int, 1>(), std::true_type());
+    else go(std::integral_constant<int, 1>(), std::false_type());
+  } else {
+    if (eq) go(std::integral_constant<int, 2>(), std::true_type());
+    else go(std::integral_constant<int, 2>(), std::false_type());
+  }
+}
+
+// Whether the staged kernels take a 3D FP32 forward solve: the single-face
+// CPML form (or none), TMA plane coordinates inside int32, and the driver's
+// tensor-map encoder available.
 bool k3t_usable(const Grid& g, const int* p, bool has_cpml) {
-  if (g_opt.tma == 0 || (g_opt.tma < 0 && !env_flag("DEEPGPR_B200_TMA"))) return false;
   if (has_cpml && !k3_cpml_single(g, p)) return false;
   if ((long long)g.nshot * g.NX >= (1LL << 31)) return false;
   return encode_tiled_fn() != nullptr;
@@ -1496,7 +1646,22 @@ void forward_impl(const ForwardCall<T>& fc) {
       ok = k3_alloc_pack(scratch, g, kg, cm, st, kf, fc.Ex, fc.Ey, fc.Ez, fc.Hx, fc.Hy, fc.Hz);
     }
     // TMA-staged kernels for the FP32 3D forward (the z-streamed kernels otherwise)
-    const bool fast3 = sizeof(T) == 4 && ok && !tm2d && k3t_usable(g, cm.p, a.has_cpml != 0);
+    const int fam3 = k3_family();
+    const bool fast3 = sizeof(T) == 4 && ok && !tm2d && fam3 == 1 && k3t_usable(g, cm.p, a.has_cpml != 0);
+    // wide kernels (fdtd_3d_wide.cuh) for the FP32 3D forward
+    const bool wide3 = sizeof(T) == 4 && ok && !tm2d && !fast3 && fam3 == 2 && k3w_usable(g, cm.p, a.has_cpml != 0, R) &&
+                       k3w_ready();
+    K3WGeom kwg;
+    memset(&kwg, 0, sizeof(kwg));
+    if (wide3) {
+      kwg = k3w_layout(g, kg.zp);
+      kwg.src_rows = src_rows;
+      kwg.rcv_rows = rcv_rows;
+      for (int ax = 0; ax < 3; ++ax) {
+        kwg.lo[ax] = kg.fr.lo[ax];
+        kwg.hi[ax] = kg.fr.hi[ax];
+      }
+    }
     K3TGeom ktg;
     memset(&ktg, 0, sizeof(ktg));
     K3TMaps kmH, kmE;
@@ -1532,8 +1697,13 @@ void forward_impl(const ForwardCall<T>& fc) {
         b.a.k_in_chunk = k;
         if (tm2d) {
           timed(KK_FWD_H, st, [&] {
-            return split_launch(
+            return tm_launch(
                 st, ss, pH,
+                [&](dim3 gfu, unsigned nfb) {
+                  if (R == 1) tmf_fwd_h<T, 1><<<gfu, wblock, 0, st>>>(b, tf, pH.frame, pH.interior, nfb);
+                  else if (R == 2) tmf_fwd_h<T, 2><<<gfu, wblock, 0, st>>>(b, tf, pH.frame, pH.interior, nfb);
+                  else tmf_fwd_h<T, 4><<<gfu, wblock, 0, st>>>(b, tf, pH.frame, pH.interior, nfb);
+                },
                 [&](cudaStream_t q, const TmGeom& fg) {
                   const dim3 gf = tm_grid(fg);
                   if (R == 1) tm_fwd_h<T, 1><<<gf, wblock, 0, q>>>(b, tf, fg);
@@ -1548,8 +1718,13 @@ void forward_impl(const ForwardCall<T>& fc) {
                 });
           });
           timed(KK_FWD_E, st, [&] {
-            return split_launch(
+            return tm_launch(
                 st, ss, pE,
+                [&](dim3 gfu, unsigned nfb) {
+                  if (R == 1) tmf_fwd_e<T, 1><<<gfu, wblock, 0, st>>>(b, tf, pE.frame, pE.interior, nfb);
+                  else if (R == 2) tmf_fwd_e<T, 2><<<gfu, wblock, 0, st>>>(b, tf, pE.frame, pE.interior, nfb);
+                  else tmf_fwd_e<T, 4><<<gfu, wblock, 0, st>>>(b, tf, pE.frame, pE.interior, nfb);
+                },
                 [&](cudaStream_t q, const TmGeom& fg) {
                   const dim3 gf = tm_grid(fg);
                   if (R == 1) tm_fwd_e<T, 1><<<gf, wblock, 0, q>>>(b, tf, fg);
@@ -1567,6 +1742,21 @@ void forward_impl(const ForwardCall<T>& fc) {
           if constexpr (sizeof(T) == 4) {
             timed(KK_FWD_H, st, [&] { k3t_launch<false>(R, eq3, st, kmH, b, kf, ktg); });
             timed(KK_FWD_E, st, [&] { k3t_launch<true>(R, eq3, st, kmE, b, kf, ktg); });
+          }
+        } else if (wide3) {
+          if constexpr (sizeof(T) == 4) {
+            timed(KK_FWD_H, st, [&] { k3w_launch<0>(R, eq3, st, b, kf, kwg); });
+            if (cpm_e == kCpmPass) {
+              const dim3 gfr((kg.fr.cum[5] + kBlock - 1) / kBlock, (unsigned)g.nshot);
+              timed(KK_FWD_E, st, [&] {
+                k3w_launch<2>(R, eq3, st, b, kf, kwg);
+                if (R == 1) k3p_fwd_e<T, 1><<<gfr, kBlock, 0, st>>>(b, kf, kg);
+                else k3p_fwd_e<T, 2><<<gfr, kBlock, 0, st>>>(b, kf, kg);
+                return 2;
+              });
+            } else {
+              timed(KK_FWD_E, st, [&] { k3w_launch<1>(R, eq3, st, b, kf, kwg); });
+            }
           }
         } else {
           const dim3 g3((unsigned)kg.nblocks), b3(32, K3_WARPS);
@@ -2000,8 +2190,13 @@ void backward_impl(const BackwardCall<T>& bc) {
         }
         if (tm2d) {
           timed(KK_ADJ_E, st, [&] {
-            return split_launch(
+            return tm_launch(
                 st, ss, pE,
+                [&](dim3 gfu, unsigned nfb) {
+                  if (R == 1) tmf_adj_e<T, 1><<<gfu, wblock, 0, st>>>(b, tl, pE.frame, pE.interior, nfb);
+                  else if (R == 2) tmf_adj_e<T, 2><<<gfu, wblock, 0, st>>>(b, tl, pE.frame, pE.interior, nfb);
+                  else tmf_adj_e<T, 4><<<gfu, wblock, 0, st>>>(b, tl, pE.frame, pE.interior, nfb);
+                },
                 [&](cudaStream_t q, const TmGeom& fg) {
                   const dim3 gf = tm_grid(fg);
                   if (R == 1) tm_adj_e<T, 1><<<gf, wblock, 0, q>>>(b, tl, fg);
@@ -2016,8 +2211,13 @@ void backward_impl(const BackwardCall<T>& bc) {
                 });
           });
           timed(KK_ADJ_H, st, [&] {
-            return split_launch(
+            return tm_launch(
                 st, ss, pH,
+                [&](dim3 gfu, unsigned nfb) {
+                  if (R == 1) tmf_adj_h<T, 1><<<gfu, wblock, 0, st>>>(b, tl, pH.frame, pH.interior, nfb);
+                  else if (R == 2) tmf_adj_h<T, 2><<<gfu, wblock, 0, st>>>(b, tl, pH.frame, pH.interior, nfb);
+                  else tmf_adj_h<T, 4><<<gfu, wblock, 0, st>>>(b, tl, pH.frame, pH.interior, nfb);
+                },
                 [&](cudaStream_t q, const TmGeom& fg) {
                   const dim3 gf = tm_grid(fg);
                   if (R == 1) tm_adj_h<T, 1, false><<<gf, wblock, 0, q>>>(b, tl, fg);
@@ -2323,13 +2523,15 @@ DGB_API int dgb_check_fixed_division(float divisor, unsigned long long* mismatch
 }
 
 // Scratch retention: the solver's per-call scratch comes from the current
-// device's default stream-ordered memory pool, which by default returns freed
-// memory to the system at every synchronisation.  A long-running caller that
-// solves back to back (a serving loop) keeps up to `bytes` cached in the pool
-// instead (-1: no limit); 0 restores the default and trims the pool.
+// device's default stream-ordered memory pool.  The library keeps up to
+// min(4 GiB, 1/32 of the device memory) of freed scratch cached in it (see
+// default_retention); a caller sets `bytes` instead (-1: no limit; 0: the
+// CUDA default, every synchronisation returns freed memory to the system,
+// and the pool is trimmed now).
 DGB_API int dgb_set_scratch_retention(long long bytes) {
   int dev = 0;
   if (!cuda_ok(cudaGetDevice(&dev), "dgb_set_scratch_retention: device")) return -1;
+  if (dev >= 0 && dev < kMaxDevices) g_retention_set[dev] = true;
   cudaMemPool_t pool;
   if (!cuda_ok(cudaDeviceGetDefaultMemPool(&pool, dev), "dgb_set_scratch_retention: pool")) return -1;
   unsigned long long v = bytes < 0 ? ~0ULL : (unsigned long long)bytes;   // the attribute is a 64-bit unsigned

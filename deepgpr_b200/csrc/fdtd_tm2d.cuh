@@ -80,11 +80,12 @@ struct WarpPos {
 
 // Warp w -> (rectangle, strip, chunk, shot), strip fastest, so the warps of
 // a CTA are neighbouring strips of the same rows.
-__device__ __forceinline__ WarpPos warp_pos(const TmGeom& tg, int nshot) {
+// blk: the CTA's index within this geometry's part of the launch.
+__device__ __forceinline__ WarpPos warp_pos(const TmGeom& tg, int nshot, unsigned blk) {
   WarpPos p;
   p.lane = threadIdx.x;
   // warp counts stay below 2^31 (checked on the host): 32-bit index arithmetic
-  const unsigned w = blockIdx.x * TM_WARPS + threadIdx.y;
+  const unsigned w = blk * TM_WARPS + threadIdx.y;
   p.live = w < (unsigned)tg.nwarps;
   TmRect rc = tg.rect[0];
 #pragma unroll
@@ -253,12 +254,17 @@ __device__ __forceinline__ void tm_fwd_h_body(const TiledFwd<T>& P, const TmBuf<
 }
 
 template <typename T, int R>
-__global__ void __launch_bounds__(32 * TM_WARPS) tm_fwd_h(TiledFwd<T> P, TmBuf<T> f, TmGeom tg) {
-  const WarpPos wp = warp_pos(tg, P.a.g.nshot);
+__device__ __forceinline__ void tm_fwd_h_run(const TiledFwd<T>& P, const TmBuf<T>& f, const TmGeom& tg, unsigned blk) {
+  const WarpPos wp = warp_pos(tg, P.a.g.nshot, blk);
   if (!wp.live) return;
   if (wp.kind == kFrameXLean) tm_fwd_h_body<T, R, kFrameXLean>(P, f, tg, wp);
   else if (wp.kind == kFrameYLean) tm_fwd_h_body<T, R, kFrameYLean>(P, f, tg, wp);
   else tm_fwd_h_body<T, R, kFrameGeneral>(P, f, tg, wp);
+}
+
+template <typename T, int R>
+__global__ void __launch_bounds__(32 * TM_WARPS) tm_fwd_h(TiledFwd<T> P, TmBuf<T> f, TmGeom tg) {
+  tm_fwd_h_run<T, R>(P, f, tg, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -405,12 +411,17 @@ __device__ __forceinline__ void tm_fwd_e_body(const TiledFwd<T>& P, const TmBuf<
 }
 
 template <typename T, int R>
-__global__ void __launch_bounds__(32 * TM_WARPS) tm_fwd_e(TiledFwd<T> P, TmBuf<T> f, TmGeom tg) {
-  const WarpPos wp = warp_pos(tg, P.a.g.nshot);
+__device__ __forceinline__ void tm_fwd_e_run(const TiledFwd<T>& P, const TmBuf<T>& f, const TmGeom& tg, unsigned blk) {
+  const WarpPos wp = warp_pos(tg, P.a.g.nshot, blk);
   if (!wp.live) return;
   if (wp.kind == kFrameXLean) tm_fwd_e_body<T, R, kFrameXLean>(P, f, tg, wp);
   else if (wp.kind == kFrameYLean) tm_fwd_e_body<T, R, kFrameYLean>(P, f, tg, wp);
   else tm_fwd_e_body<T, R, kFrameGeneral>(P, f, tg, wp);
+}
+
+template <typename T, int R>
+__global__ void __launch_bounds__(32 * TM_WARPS) tm_fwd_e(TiledFwd<T> P, TmBuf<T> f, TmGeom tg) {
+  tm_fwd_e_run<T, R>(P, f, tg, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -561,9 +572,9 @@ __device__ __forceinline__ void tm_adj_e_body(const TiledAdj<T>& P, const TmBuf<
 }
 
 template <typename T, int R>
-__global__ void __launch_bounds__(32 * TM_WARPS) tm_adj_e(TiledAdj<T> P, TmBuf<T> t, TmGeom tg) {
+__device__ __forceinline__ void tm_adj_e_run(const TiledAdj<T>& P, const TmBuf<T>& t, const TmGeom& tg, unsigned blk) {
   const AdjArgs<T>& a = P.a;
-  if (a.want_src && tg.sum_source && blockIdx.x == 0 && threadIdx.y == 0) {
+  if (a.want_src && tg.sum_source && blk == 0 && threadIdx.y == 0) {
     // waveform gradient of step it: shots summed in order (deepgpr_cpu.c:1524-1533)
     const int it = a.ctrl->cur - a.k_in_chunk;
     for (int m = threadIdx.x; m < a.nsrc; m += 32) {
@@ -572,11 +583,16 @@ __global__ void __launch_bounds__(32 * TM_WARPS) tm_adj_e(TiledAdj<T> P, TmBuf<T
       a.grad_source[(long long)m * a.nt + it] = acc;
     }
   }
-  const WarpPos wp = warp_pos(tg, a.g.nshot);
+  const WarpPos wp = warp_pos(tg, a.g.nshot, blk);
   if (!wp.live) return;
   if (wp.kind == kFrameXLean) tm_adj_e_body<T, R, kFrameXLean>(P, t, tg, wp);
   else if (wp.kind == kFrameYLean) tm_adj_e_body<T, R, kFrameYLean>(P, t, tg, wp);
   else tm_adj_e_body<T, R, kFrameGeneral>(P, t, tg, wp);
+}
+
+template <typename T, int R>
+__global__ void __launch_bounds__(32 * TM_WARPS) tm_adj_e(TiledAdj<T> P, TmBuf<T> t, TmGeom tg) {
+  tm_adj_e_run<T, R>(P, t, tg, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -721,8 +737,8 @@ __device__ __forceinline__ void tm_adj_h_body(const TiledAdj<T>& P, const TmBuf<
 }
 
 template <typename T, int R, bool PROLOGUE>
-__global__ void __launch_bounds__(32 * TM_WARPS) tm_adj_h(TiledAdj<T> P, TmBuf<T> t, TmGeom tg) {
-  const WarpPos wp = warp_pos(tg, P.a.g.nshot);
+__device__ __forceinline__ void tm_adj_h_run(const TiledAdj<T>& P, const TmBuf<T>& t, const TmGeom& tg, unsigned blk) {
+  const WarpPos wp = warp_pos(tg, P.a.g.nshot, blk);
   if (!wp.live) return;
   if (PROLOGUE) {
     tm_adj_h_body<T, R, true, kFrameGeneral>(P, t, tg, wp);
@@ -731,6 +747,11 @@ __global__ void __launch_bounds__(32 * TM_WARPS) tm_adj_h(TiledAdj<T> P, TmBuf<T
     else if (wp.kind == kFrameYLean) tm_adj_h_body<T, R, false, kFrameYLean>(P, t, tg, wp);
     else tm_adj_h_body<T, R, false, kFrameGeneral>(P, t, tg, wp);
   }
+}
+
+template <typename T, int R, bool PROLOGUE>
+__global__ void __launch_bounds__(32 * TM_WARPS) tm_adj_h(TiledAdj<T> P, TmBuf<T> t, TmGeom tg) {
+  tm_adj_h_run<T, R, PROLOGUE>(P, t, tg, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -944,12 +965,12 @@ __device__ __forceinline__ float tile8_absmax(float v) {
 
 // Interior forward H.
 template <typename T, int R>
-__global__ void __launch_bounds__(32 * TM_WARPS) tmi_fwd_h(TiledFwd<T> P, TmBuf<T> f, TmGeom tg) {
+__device__ __forceinline__ void tmi_fwd_h_run(const TiledFwd<T>& P, const TmBuf<T>& f, const TmGeom& tg, unsigned blk) {
   constexpr int MLO = -(R - 1), MHI = R + 3, NM = MHI - MLO + 1;
   const FwdArgs<T>& a = P.a;
   const Grid& g = a.g;
   const int NX = g.NX, NY = g.NY, NYP = tg.NYP;
-  const WarpPos wp = warp_pos(tg, g.nshot);
+  const WarpPos wp = warp_pos(tg, g.nshot, blk);
   if (!wp.live) return;
   const int lane = wp.lane, s = wp.s, x0 = wp.x0, x1 = wp.x1;
   const int j = wp.base + 4 * lane;
@@ -1041,12 +1062,12 @@ __global__ void __launch_bounds__(32 * TM_WARPS) tmi_fwd_h(TiledFwd<T> P, TmBuf<
 // Interior forward E (+ R^n history).  Rows holding sources or receivers are
 // frame rows.
 template <typename T, int R>
-__global__ void __launch_bounds__(32 * TM_WARPS) tmi_fwd_e(TiledFwd<T> P, TmBuf<T> f, TmGeom tg) {
+__device__ __forceinline__ void tmi_fwd_e_run(const TiledFwd<T>& P, const TmBuf<T>& f, const TmGeom& tg, unsigned blk) {
   constexpr int MLO = -R, MHI = R + 2, NM = MHI - MLO + 1;
   const FwdArgs<T>& a = P.a;
   const Grid& g = a.g;
   const int NX = g.NX, NY = g.NY, NYP = tg.NYP;
-  const WarpPos wp = warp_pos(tg, g.nshot);
+  const WarpPos wp = warp_pos(tg, g.nshot, blk);
   if (!wp.live) return;
   const int lane = wp.lane, s = wp.s, x0 = wp.x0, x1 = wp.x1;
   const int j = wp.base + 4 * lane;
@@ -1143,12 +1164,12 @@ __global__ void __launch_bounds__(32 * TM_WARPS) tmi_fwd_e(TiledFwd<T> P, TmBuf<
 
 // Interior adjoint E step.
 template <typename T, int R>
-__global__ void __launch_bounds__(32 * TM_WARPS) tmi_adj_e(TiledAdj<T> P, TmBuf<T> t, TmGeom tg) {
+__device__ __forceinline__ void tmi_adj_e_run(const TiledAdj<T>& P, const TmBuf<T>& t, const TmGeom& tg, unsigned blk) {
   constexpr int MLO = -(R - 1), MHI = R + 3, NM = MHI - MLO + 1;
   const AdjArgs<T>& a = P.a;
   const Grid& g = a.g;
   const int NX = g.NX, NY = g.NY, NYP = tg.NYP;
-  const WarpPos wp = warp_pos(tg, g.nshot);
+  const WarpPos wp = warp_pos(tg, g.nshot, blk);
   if (!wp.live) return;
   const int lane = wp.lane, s = wp.s, x0 = wp.x0, x1 = wp.x1;
   const int j = wp.base + 4 * lane;
@@ -1223,12 +1244,12 @@ __global__ void __launch_bounds__(32 * TM_WARPS) tmi_adj_e(TiledAdj<T> P, TmBuf<
 // Interior adjoint H step.  Rows holding receivers or sources are frame rows
 // (the head of step it-1 has nothing else to do in the interior).
 template <typename T, int R>
-__global__ void __launch_bounds__(32 * TM_WARPS) tmi_adj_h(TiledAdj<T> P, TmBuf<T> t, TmGeom tg) {
+__device__ __forceinline__ void tmi_adj_h_run(const TiledAdj<T>& P, const TmBuf<T>& t, const TmGeom& tg, unsigned blk) {
   constexpr int MLO = -R, MHI = R + 2, NM = MHI - MLO + 1;
   const AdjArgs<T>& a = P.a;
   const Grid& g = a.g;
   const int NX = g.NX, NY = g.NY, NYP = tg.NYP;
-  const WarpPos wp = warp_pos(tg, g.nshot);
+  const WarpPos wp = warp_pos(tg, g.nshot, blk);
   if (!wp.live) return;
   const int lane = wp.lane, s = wp.s, x0 = wp.x0, x1 = wp.x1;
   const int j = wp.base + 4 * lane;
@@ -1297,6 +1318,69 @@ __global__ void __launch_bounds__(32 * TM_WARPS) tmi_adj_h(TiledAdj<T> P, TmBuf<
 #pragma unroll
       for (int e = 0; e < 4; ++e) qA[m][e] = qA[m + 1][e];
   }
+}
+
+#define DG_TMI_WRAPPER(NAME, ARGS, BUF)                                                               \
+  template <typename T, int R>                                                                       \
+  __global__ void __launch_bounds__(32 * TM_WARPS) NAME(ARGS<T> P, TmBuf<T> t, TmGeom tg) {          \
+    NAME##_run<T, R>(P, t, tg, blockIdx.x);                                                          \
+  }
+DG_TMI_WRAPPER(tmi_fwd_h, TiledFwd, f)
+DG_TMI_WRAPPER(tmi_fwd_e, TiledFwd, f)
+DG_TMI_WRAPPER(tmi_adj_e, TiledAdj, t)
+DG_TMI_WRAPPER(tmi_adj_h, TiledAdj, t)
+#undef DG_TMI_WRAPPER
+
+// ---------------------------------------------------------------------------
+// Fused half steps: one launch of nfb frame CTAs (the general kernels on the
+// frame geometry fg) and gridDim.x - nfb interior CTAs (the interior kernels
+// on ig), dealt evenly through the launch: CTA b is a frame CTA when
+// floor((b+1) nfb / n) > floor(b nfb / n), n = gridDim.x.  The CTAs of a launch
+// start in index order, so every SM runs the frame's latency-bound warps
+// beside the interior's bandwidth-bound ones, where two launches on two
+// streams mostly ran one after the other.  The two parts touch disjoint
+// cells and read only fields the half step does not write.
+// ---------------------------------------------------------------------------
+struct FusedBlock {
+  bool frame;
+  unsigned idx;   // CTA index within its part
+};
+__device__ __forceinline__ FusedBlock fused_block(unsigned nfb) {
+  const unsigned long long b = blockIdx.x, n = gridDim.x;
+  const unsigned f1 = (unsigned)((b + 1) * nfb / n), f0 = (unsigned)(b * nfb / n);
+  FusedBlock r;
+  r.frame = f1 > f0;
+  r.idx = r.frame ? f0 : (unsigned)b - f1;
+  return r;
+}
+
+template <typename T, int R>
+__global__ void __launch_bounds__(32 * TM_WARPS) tmf_fwd_h(TiledFwd<T> P, TmBuf<T> f, TmGeom fg, TmGeom ig,
+                                                           unsigned nfb) {
+  const FusedBlock fb = fused_block(nfb);
+  if (fb.frame) tm_fwd_h_run<T, R>(P, f, fg, fb.idx);
+  else tmi_fwd_h_run<T, R>(P, f, ig, fb.idx);
+}
+template <typename T, int R>
+__global__ void __launch_bounds__(32 * TM_WARPS) tmf_fwd_e(TiledFwd<T> P, TmBuf<T> f, TmGeom fg, TmGeom ig,
+                                                           unsigned nfb) {
+  const FusedBlock fb = fused_block(nfb);
+  if (fb.frame) tm_fwd_e_run<T, R>(P, f, fg, fb.idx);
+  else tmi_fwd_e_run<T, R>(P, f, ig, fb.idx);
+}
+template <typename T, int R>
+__global__ void __launch_bounds__(32 * TM_WARPS) tmf_adj_e(TiledAdj<T> P, TmBuf<T> t, TmGeom fg, TmGeom ig,
+                                                           unsigned nfb) {
+  const FusedBlock fb = fused_block(nfb);
+  if (fb.frame) tm_adj_e_run<T, R>(P, t, fg, fb.idx);
+  else tmi_adj_e_run<T, R>(P, t, ig, fb.idx);
+}
+template <typename T, int R>
+__global__ void __launch_bounds__(32 * TM_WARPS) tmf_adj_h(TiledAdj<T> P, TmBuf<T> t, TmGeom fg, TmGeom ig,
+                                                           unsigned nfb) {
+  const FusedBlock fb = fused_block(nfb);
+  if (fb.frame) tm_adj_h_run<T, R, false>(P, t, fg, fb.idx);
+  else tmi_adj_h_run<T, R>(P, t, ig, fb.idx);
 }
 
 // (nshot, NX, NY, 2) plane k = 0  <->  (nshot, NX, NYP) with zero padding.

@@ -135,7 +135,9 @@ def profile_read() -> Dict[str, Tuple[float, int]]:
 
 def set_scratch_retention(nbytes: int) -> None:
     """Keep up to ``nbytes`` of the solver's freed scratch cached on the current
-    device (-1: no limit, 0: the default, trimmed); see ``dgb_set_scratch_retention``."""
+    device (-1: no limit; 0: none, the CUDA default, and trim now).  Without a
+    call the library keeps min(4 GiB, 1/32 of the device memory); see
+    ``dgb_set_scratch_retention``."""
     lib = load_library()
     if lib.dgb_set_scratch_retention(int(nbytes)) != 0:
         raise NativeLibraryError(last_error(lib) or "dgb_set_scratch_retention failed")

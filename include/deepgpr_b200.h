@@ -186,12 +186,14 @@ int dgb_check_fixed_division(float divisor, unsigned long long* mismatches, unsi
 
 /* No counterpart in the reference.  The solver's per-call device scratch
  * (working copies, point tables, CPML weights) comes from the current device's
- * default stream-ordered memory pool, which by default gives freed memory
- * back at every synchronisation, so every call maps its scratch again.  A
- * caller that solves back to back -- a serving loop -- keeps up to `bytes`
- * cached in the pool (-1: no limit); 0 restores the default and trims the
- * pool.  Affects every stream-ordered allocation of the process on that
- * device.  Returns 0, or -1 with deepgpr_last_error() set. */
+ * default stream-ordered memory pool.  With the CUDA default the pool gives
+ * freed memory back at every synchronisation and every call maps its scratch
+ * again (on virtualised hosts such mappings stalled back-to-back solves by
+ * up to 0.6 s), so on first use of a device the library keeps up to
+ * min(4 GiB, 1/32 of the device memory) cached.  A caller sets the amount
+ * instead: `bytes` (-1: no limit; 0: the CUDA default, and the pool is
+ * trimmed now).  Affects every stream-ordered allocation of the process on
+ * that device.  Returns 0, or -1 with deepgpr_last_error() set. */
 int dgb_set_scratch_retention(long long bytes);
 
 /* No counterpart in the reference.  Launch-shape choices for the calling
