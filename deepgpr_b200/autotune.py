@@ -9,7 +9,7 @@ history format, precision):
 * 2D TM: interior row chunks (``tm_chunks``), frame rows per warp chunk
   (``tm_frame_rows``), time steps per captured graph (``chunk``);
 * 3D: x chunks of the streamed kernels (``k3_xchunks``), the forward kernel
-  family (z-streamed or TMA-staged, FP32), time steps per graph.
+  family (FP32: 2 wide, 0 z-streamed, 1 TMA-staged), time steps per graph.
 
 The knobs change how the work is split, never what is computed, so results
 are the same for every choice.  A probe is a forward solve without history
@@ -49,7 +49,7 @@ def search_space(cfg) -> List[Tuple[str, Sequence[int]]]:
         return [("tm_chunks", (0, 1, 2, 4, 8)), ("tm_frame_rows", (0, 4, 16)), ("chunk", (16, 32))]
     space: List[Tuple[str, Sequence[int]]] = [("k3_xchunks", (0, 1, 2, 4, 8, 16))]
     if cfg.dtype == torch.float32:
-        space.append(("tma", (0, 1)))
+        space.append(("tma", (2, 0, 1)))
     space.append(("chunk", (16, 32)))
     return space
 

@@ -198,8 +198,9 @@ int dgb_set_scratch_retention(long long bytes);
 
 /* No counterpart in the reference.  Launch-shape choices for the calling
  * thread's next solves (set by deepgpr_b200.autotune): 2D interior row
- * chunks, 2D frame rows per warp chunk, 3D x chunks, 3D forward kernel family
- * (1 TMA-staged, 0 z-streamed, -1 the DEEPGPR_B200_TMA environment choice).
+ * chunks, 2D frame rows per warp chunk, 3D x chunks, 3D FP32 forward kernel
+ * family (2 wide, 1 TMA-staged, 0 z-streamed; -1 the environment choice:
+ * DEEPGPR_B200_TMA=1 staged, DEEPGPR_B200_NARROW=1 z-streamed, else wide).
  * 0 / -1 restore the built-in heuristics; results do not depend on them.
  * Returns 0, or -1 for out-of-range values. */
 int dgb_set_tuning(int tm_chunks, int tm_frame_rows, int k3_xchunks, int tma);

@@ -1,7 +1,8 @@
 """The launch-shape autotuner: a tuned solve equals the default one, and the choice is kept.
 
 The autotuner's knobs (2D interior row chunks and frame rows, 3D x chunks,
-the 3D forward kernel family, time steps per graph) split the same work
+the 3D forward kernel family -- wide, z-streamed or TMA-staged --, time steps
+per graph) split the same work
 differently; every cell still evaluates the same expressions in the same
 order, so receivers, states and gradients are bit for bit those of the
 default launch shapes.
@@ -48,7 +49,8 @@ def test_every_3d_launch_choice_gives_the_same_receivers(cuda_device):
     p = problem_3d(nt=40, order=4, shape=(40, 36, 70), pml=4)
     ref = run_product(p, cuda_device, backward=False)["receivers"]
     real = native.invoke
-    for tuning, chunk in (((0, 0, 1, 0), 16), ((0, 0, 5, 0), 8), ((0, 0, 0, 1), 16), ((0, 0, 3, 1), 32)):
+    for tuning, chunk in (((0, 0, 1, 0), 16), ((0, 0, 5, 0), 8), ((0, 0, 0, 1), 16), ((0, 0, 3, 1), 32),
+                          ((0, 0, 0, 2), 16), ((0, 0, 3, 2), 8), ((0, 0, 1, 2), 32)):
         def spy(name, args, **opts):
             opts = dict(opts, tuning=tuning, chunk=chunk)
             return real(name, args, **opts)
