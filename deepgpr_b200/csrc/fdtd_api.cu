@@ -28,6 +28,7 @@
 #include "fdtd_3d_adj.cuh"
 #include "fdtd_3d_fast.cuh"
 #include "fdtd_3d_wide.cuh"
+#include "fdtd_3d_wide_adj.cuh"
 
 #define DGB_API extern "C" __attribute__((visibility("default")))
 
@@ -1306,6 +1307,41 @@ bool k3w_ready_r() {
 // launches may be captured into graphs).
 bool k3w_ready() { return k3w_ready_r<1>() && k3w_ready_r<2>(); }
 
+template <int R, bool EQ>
+bool k3w_adj_prepare() {
+  static const bool ok =
+      cudaFuncSetAttribute(k3w_adj_e<R, EQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, kw_adj_smem_bytes()) ==
+          cudaSuccess &&
+      cudaFuncSetAttribute(k3w_adj_h<R, EQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, kw_adj_smem_bytes()) ==
+          cudaSuccess;
+  return ok;
+}
+bool k3w_adj_ready() {
+  return k3w_adj_prepare<1, true>() && k3w_adj_prepare<1, false>() && k3w_adj_prepare<2, true>() &&
+         k3w_adj_prepare<2, false>();
+}
+
+// The wide adjoint kernels: KIND 0 the adjoint E step, 1 the adjoint H step.
+template <int KIND>
+void k3w_adj_launch(int R, bool eq, cudaStream_t st, const TiledAdj<float>& P, const K3Buf<float>& kf,
+                    const K3WGeom& kg) {
+  const dim3 grid((unsigned)kg.nblocks), block(32, KW_WARPS);
+  const int bytes = kw_adj_smem_bytes();
+  auto go = [&](auto RR, auto E) {
+    constexpr int RV = decltype(RR)::value;
+    constexpr bool EV = decltype(E)::value;
+    if constexpr (KIND == 0) k3w_adj_e<RV, EV><<<grid, block, bytes, st>>>(P, kf, kg);
+    else k3w_adj_h<RV, EV><<<grid, block, bytes, st>>>(P, kf, kg);
+  };
+  if (R == 1) {
+    if (eq) go(std::integral_constant<int, 1>(), std::true_type());
+    else go(std::integral_constant<int, 1>(), std::false_type());
+  } else {
+    if (eq) go(std::integral_constant<int, 2>(), std::true_type());
+    else go(std::integral_constant<int, 2>(), std::false_type());
+  }
+}
+
 K3WGeom k3w_layout(const Grid& g, int zp) {
   K3WGeom kg;
   memset(&kg, 0, sizeof(kg));
@@ -2128,6 +2164,16 @@ void backward_impl(const BackwardCall<T>& bc) {
     const bool eq3 = cm.dy == cm.dx && cm.dz == cm.dx;
     // general CPML form where faces of an axis may meet, or past the z-face pass's grid limit
     const bool gen3 = has_cpml && (!kg.cpml_single || g.nshot > 65535);
+    // wide adjoint kernels (fdtd_3d_wide_adj.cuh) for FP32 with the single-face CPML form (or none)
+    const bool wide3 = sizeof(T) == 4 && ok && !tm2d && !gen3 && k3_family() == 2 &&
+                       k3w_usable(g, cm.p, has_cpml, R) && k3w_adj_ready();
+    K3WGeom kwg;
+    memset(&kwg, 0, sizeof(kwg));
+    if (wide3) {
+      kwg = k3w_layout(g, kg.zp);
+      kwg.src_rows = src_rows;
+      kwg.rcv_rows = rcv_rows;
+    }
     if (ok && !tm2d) {
       // the double-precision stages exceed the 48 KB default
       k3_variant<T>(R, eq3, gen3, [&](auto RR, auto E, auto G) {
@@ -2242,20 +2288,30 @@ void backward_impl(const BackwardCall<T>& bc) {
           const dim3 gph((fh.cum[5] + kBlock - 1) / kBlock, (unsigned)g.nshot);
           const dim3 gpe((fe.cum[5] + kBlock - 1) / kBlock, (unsigned)g.nshot);
           timed(KK_ADJ_E, st, [&] {
-            k3_variant<T>(R, eq3, gen3, [&](auto RR, auto E, auto G) {
-              constexpr int r = decltype(RR)::value;
-              k3v_adj_e<T, r, decltype(E)::value, decltype(G)::value>
-                  <<<nb, kblock, k3_adj_smem_bytes<T, r>(), st>>>(b, kb, kg);
-            });
+            if constexpr (sizeof(T) == 4) {
+              if (wide3) k3w_adj_launch<0>(R, eq3, st, b, kb, kwg);
+            }
+            if (!wide3) {
+              k3_variant<T>(R, eq3, gen3, [&](auto RR, auto E, auto G) {
+                constexpr int r = decltype(RR)::value;
+                k3v_adj_e<T, r, decltype(E)::value, decltype(G)::value>
+                    <<<nb, kblock, k3_adj_smem_bytes<T, r>(), st>>>(b, kb, kg);
+              });
+            }
             if (zpass) k3p_adj_w<T, false><<<gph, kBlock, 0, st>>>(b, kb, kg, fh);
             return zpass ? 2 : 1;
           });
           timed(KK_ADJ_H, st, [&] {
-            k3_variant<T>(R, eq3, gen3, [&](auto RR, auto E, auto G) {
-              constexpr int r = decltype(RR)::value;
-              k3v_adj_h<T, r, decltype(E)::value, decltype(G)::value>
-                  <<<nb, kblock, k3_adj_smem_bytes<T, r>(), st>>>(b, kb, kg);
-            });
+            if constexpr (sizeof(T) == 4) {
+              if (wide3) k3w_adj_launch<1>(R, eq3, st, b, kb, kwg);
+            }
+            if (!wide3) {
+              k3_variant<T>(R, eq3, gen3, [&](auto RR, auto E, auto G) {
+                constexpr int r = decltype(RR)::value;
+                k3v_adj_h<T, r, decltype(E)::value, decltype(G)::value>
+                    <<<nb, kblock, k3_adj_smem_bytes<T, r>(), st>>>(b, kb, kg);
+              });
+            }
             if (zpass) k3p_adj_w<T, true><<<gpe, kBlock, 0, st>>>(b, kb, kg, fe);
             return zpass ? 2 : 1;
           });
