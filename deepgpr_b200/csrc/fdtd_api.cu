@@ -1239,17 +1239,37 @@ bool env_flag(const char* name) {
   return v && v[0] && v[0] != '0';
 }
 
-// 3D FP32 forward kernel family: the tuning knob when set (0 z-streamed,
-// 1 staged, 2 wide), else DEEPGPR_B200_TMA=1 selects the staged kernels,
-// DEEPGPR_B200_NARROW=1 the z-streamed ones, and the wide ones by default
-// (measured 2-4 % faster per half step than the z-streamed kernels on
-// 320 x 320 x 160 + CPML 10, 24 % faster on the E half step without CPML).
-// A family that does not take the solve falls back to the z-streamed kernels.
+// 3D FP32 kernel family: the tuning knob when set (0 z-streamed, 1 staged
+// forward, 2 wide), else DEEPGPR_B200_TMA=1 (staged forward) or
+// DEEPGPR_B200_NARROW=1 (z-streamed), else -1: the automatic choice of
+// k3w_auto.  A family that does not take the solve falls back to the
+// z-streamed kernels.
 int k3_family() {
   if (g_opt.tma >= 0) return g_opt.tma;
   if (env_flag("DEEPGPR_B200_TMA")) return 1;
-  return env_flag("DEEPGPR_B200_NARROW") ? 0 : 2;
+  return env_flag("DEEPGPR_B200_NARROW") ? 0 : -1;
 }
+
+// Fraction of the grid's cells outside every CPML slab and the grid ends.
+double k3_interior_fraction(const Grid& g, const int* p) {
+  auto f = [](int n, int lo, int hi) { return std::max(0.0, (double)(n - lo - hi - 2) / n); };
+  return f(g.NX, p[0], p[1]) * f(g.NY, p[2], p[3]) * f(g.NZ, p[4], p[5]);
+}
+
+// Automatic family of a half step (FP32, wide kernels usable).  The wide
+// kernels need busy lanes: at least 70 % of their 128-column strips' lanes
+// hold grid columns (the z-streamed kernels use 64-column strips).  Then the
+// wide E forward step of the pass form is taken always, and the wide H
+// forward step, E forward step with its CPML in the kernel and adjoint steps
+// when at least 3/4 of the cells lie outside the CPML frame.  Measured with
+// the z-streamed kernels as the alternative: on 320 x 320 x 160 + CPML 10
+// (77 % outside, 71 % busy lanes) the wide kernels are 2-10 % faster per
+// half step; on 160 x 160 x 96 + CPML 10 (65 %, 91 %) the wide E pass-form
+// step is 17 % faster and the others 8-34 % slower (they read the x- and
+// y-face CPML operands where they are used); on 140^3 + CPML 10 (64 %, 63 %)
+// the wide E pass-form step is 6 % slower.
+double k3w_lane_use(const Grid& g) { return (double)g.NZ / (double)(((g.NZ + 31) / 32 * 32 + KWW - 1) / KWW * KWW); }
+bool k3w_auto(bool e_pass, double interior, double lanes) { return lanes >= 0.7 && (e_pass || interior >= 0.75); }
 
 // Whether the wide kernels take a 3D FP32 forward solve: radius <= 2, the
 // single-face CPML form (or none) and at most 64 z-face cells of E and of H
@@ -1687,12 +1707,16 @@ void forward_impl(const ForwardCall<T>& fc) {
     // TMA-staged kernels for the FP32 3D forward (the z-streamed kernels otherwise)
     const int fam3 = k3_family();
     const bool fast3 = sizeof(T) == 4 && ok && !tm2d && fam3 == 1 && k3t_usable(g, cm.p, a.has_cpml != 0);
-    // wide kernels (fdtd_3d_wide.cuh) for the FP32 3D forward
-    const bool wide3 = sizeof(T) == 4 && ok && !tm2d && !fast3 && fam3 == 2 && k3w_usable(g, cm.p, a.has_cpml != 0, R) &&
-                       k3w_ready();
+    // wide kernels (fdtd_3d_wide.cuh) for the FP32 3D forward half steps
+    const bool wide_ok = sizeof(T) == 4 && ok && !tm2d && !fast3 && (fam3 == 2 || fam3 < 0) &&
+                         k3w_usable(g, cm.p, a.has_cpml != 0, R) && k3w_ready();
+    const double inner3 = k3_interior_fraction(g, cm.p);
+    const double lanes3 = k3w_lane_use(g);
+    const bool wideH = wide_ok && (fam3 == 2 || k3w_auto(false, inner3, lanes3));
+    const bool wideE = wide_ok && (fam3 == 2 || k3w_auto(cpm_e == kCpmPass, inner3, lanes3));
     K3WGeom kwg;
     memset(&kwg, 0, sizeof(kwg));
-    if (wide3) {
+    if (wideH || wideE) {
       kwg = k3w_layout(g, kg.zp);
       kwg.src_rows = src_rows;
       kwg.rcv_rows = rcv_rows;
@@ -1782,27 +1806,18 @@ void forward_impl(const ForwardCall<T>& fc) {
             timed(KK_FWD_H, st, [&] { k3t_launch<false>(R, eq3, st, kmH, b, kf, ktg); });
             timed(KK_FWD_E, st, [&] { k3t_launch<true>(R, eq3, st, kmE, b, kf, ktg); });
           }
-        } else if (wide3) {
-          if constexpr (sizeof(T) == 4) {
-            timed(KK_FWD_H, st, [&] { k3w_launch<0>(R, eq3, st, b, kf, kwg); });
-            if (cpm_e == kCpmPass) {
-              const dim3 gfr((kg.fr.cum[5] + kBlock - 1) / kBlock, (unsigned)g.nshot);
-              timed(KK_FWD_E, st, [&] {
-                k3w_launch<2>(R, eq3, st, b, kf, kwg);
-                if (R == 1) k3p_fwd_e<T, 1><<<gfr, kBlock, 0, st>>>(b, kf, kg);
-                else k3p_fwd_e<T, 2><<<gfr, kBlock, 0, st>>>(b, kf, kg);
-                return 2;
-              });
-            } else {
-              timed(KK_FWD_E, st, [&] { k3w_launch<1>(R, eq3, st, b, kf, kwg); });
-            }
-          }
         } else {
           const dim3 g3((unsigned)kg.nblocks), b3(32, K3_WARPS);
           const dim3 gfr((kg.fr.cum[5] + kBlock - 1) / kBlock, (unsigned)g.nshot);
           const int nyb = (g.NY + kZfRowsF - 1) / kZfRowsF;
           const dim3 gz((unsigned)(g.NX * nyb), (unsigned)g.nshot), bz(32, kZfRowsF);
           timed(KK_FWD_H, st, [&] {
+            if constexpr (sizeof(T) == 4) {
+              if (wideH) {
+                k3w_launch<0>(R, eq3, st, b, kf, kwg);
+                return 1;
+              }
+            }
             k3_fwd_variant<T>(R, eq3, cpm_h, [&](auto RR, auto E, auto C) {
               k3v_fwd_h<T, decltype(RR)::value, decltype(E)::value, decltype(C)::value><<<g3, b3, 0, st>>>(b, kf, kg);
               if (kg.zpost_h) k3z_fwd_h<T, decltype(RR)::value><<<gz, bz, 0, st>>>(b, kf, kg, nyb);
@@ -1810,6 +1825,18 @@ void forward_impl(const ForwardCall<T>& fc) {
             return kg.zpost_h ? 2 : 1;
           });
           timed(KK_FWD_E, st, [&] {
+            if constexpr (sizeof(T) == 4) {
+              if (wideE) {
+                if (cpm_e != kCpmPass) {
+                  k3w_launch<1>(R, eq3, st, b, kf, kwg);
+                  return 1;
+                }
+                k3w_launch<2>(R, eq3, st, b, kf, kwg);
+                if (R == 1) k3p_fwd_e<T, 1><<<gfr, kBlock, 0, st>>>(b, kf, kg);
+                else k3p_fwd_e<T, 2><<<gfr, kBlock, 0, st>>>(b, kf, kg);
+                return 2;
+              }
+            }
             k3_fwd_variant<T>(R, eq3, cpm_e, [&](auto RR, auto E, auto C) {
               k3v_fwd_e<T, decltype(RR)::value, decltype(E)::value, decltype(C)::value><<<g3, b3, 0, st>>>(b, kf, kg);
               if (cpm_e == kCpmPass) k3p_fwd_e<T, decltype(RR)::value><<<gfr, kBlock, 0, st>>>(b, kf, kg);
@@ -2165,7 +2192,9 @@ void backward_impl(const BackwardCall<T>& bc) {
     // general CPML form where faces of an axis may meet, or past the z-face pass's grid limit
     const bool gen3 = has_cpml && (!kg.cpml_single || g.nshot > 65535);
     // wide adjoint kernels (fdtd_3d_wide_adj.cuh) for FP32 with the single-face CPML form (or none)
-    const bool wide3 = sizeof(T) == 4 && ok && !tm2d && !gen3 && k3_family() == 2 &&
+    const int fam3 = k3_family();
+    const bool wide3 = sizeof(T) == 4 && ok && !tm2d && !gen3 && (fam3 == 2 || fam3 < 0) &&
+                       (fam3 == 2 || k3w_auto(false, k3_interior_fraction(g, cm.p), k3w_lane_use(g))) &&
                        k3w_usable(g, cm.p, has_cpml, R) && k3w_adj_ready();
     K3WGeom kwg;
     memset(&kwg, 0, sizeof(kwg));
