@@ -34,7 +34,7 @@ import torch
 from . import native
 from .storage import encode_storage_type
 
-DEFAULT = {"tm_chunks": 0, "tm_frame_rows": 0, "k3_xchunks": 0, "tma": -1, "chunk": 16}
+DEFAULT = {"tm_chunks": 0, "tm_frame_rows": 0, "k3_xchunks": 0, "tma": -1, "chunk": 32}
 
 
 def signature(cfg) -> str:
@@ -46,11 +46,11 @@ def signature(cfg) -> str:
 def search_space(cfg) -> List[Tuple[str, Sequence[int]]]:
     """Coordinates searched in turn (the first value of each is the default)."""
     if cfg.tm2d:
-        return [("tm_chunks", (0, 1, 2, 4, 8)), ("tm_frame_rows", (0, 4, 16)), ("chunk", (16, 32))]
+        return [("tm_chunks", (0, 1, 2, 4, 8)), ("tm_frame_rows", (0, 4, 8, 32)), ("chunk", (32, 16, 64))]
     space: List[Tuple[str, Sequence[int]]] = [("k3_xchunks", (0, 1, 2, 4, 8, 16))]
     if cfg.dtype == torch.float32:
         space.append(("tma", (2, 0, 1)))
-    space.append(("chunk", (16, 32)))
+    space.append(("chunk", (32, 16, 64)))
     return space
 
 

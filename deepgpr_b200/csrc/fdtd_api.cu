@@ -50,7 +50,7 @@ struct ThreadOptions {
   cudaStream_t user_stream = nullptr;  // nullptr: legacy default stream
   bool user_stream_set = false;
   int acc64 = 1;          // FP64 accumulation of the material gradient
-  int chunk = 16;         // time steps per launch chunk
+  int chunk = 32;         // time steps per launch chunk
   int use_graph = 1;      // capture a chunk into a CUDA graph and replay it
   int order_override = 0; // per-thread FDTD order (0: use the global)
   // launch-shape choices of the autotuner (0 / -1: the built-in heuristics)
@@ -533,7 +533,7 @@ void tm_add_rect(TmGeom& tg, int nshot, int seg0, int nseg, int width, int row0,
 // (occupancy `iblocks` CTAs per SM, chunks of at least 16 rows).  The frame
 // is split by kind (see kFrameGeneral): edge tiles on x-lean rows, edge tiles
 // elsewhere (corners, chunks of 2 rows), and interior tiles on the remaining
-// rows (chunks of 8 rows), all in one launch.
+// rows (chunks of 16 rows), all in one launch.
 struct TmPlan {
   TmGeom interior, frame;
 };
@@ -596,7 +596,7 @@ TmPlan tm_plan(const TmGeom& base, const Grid& g, int kind, int R, const TmFaces
   const auto xg = complement(g.NX, xl);
   const auto mid = complement(g.NX, rows);
   const bool fits = 2 * xl.size() + 2 * xg.size() + mid.size() <= (size_t)kTmMaxRects;
-  const int frame_xc = g_opt.tm_frame_rows > 0 ? g_opt.tm_frame_rows : 8, corner_xc = 2;
+  const int frame_xc = g_opt.tm_frame_rows > 0 ? g_opt.tm_frame_rows : 16, corner_xc = 2;
   if (!rows.empty() && thi > tlo && fits) {
     const int n128 = (thi - tlo + 3) / 4;
     int nrows = 0;

@@ -279,7 +279,7 @@ DEFAULT_TUNING = (0, 0, 0, -1)
 
 
 def invoke(name: str, args: Mapping[str, Any], *, fdtd_order: int, stream: Any = None,
-           acc64: bool = True, chunk: int = 16, use_graph: bool = True,
+           acc64: bool = True, chunk: int = 32, use_graph: bool = True,
            tuning: Sequence[int] = DEFAULT_TUNING) -> None:
     """Call ``forward``/``backward`` (or their FP64 twins) on ``stream``.
 

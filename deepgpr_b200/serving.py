@@ -19,7 +19,7 @@ requests keeps allocating (and synchronising the device).
 Each slot is a host thread with its own CUDA stream; inside the native library
 every host thread has its own work and side streams.  The kernels of all
 admitted requests therefore run concurrently on the GPU, and every solve's time
-loop is replayed from CUDA graphs captured per 16-step chunk.  Gradient solves
+loop is replayed from CUDA graphs captured per 32-step chunk.  Gradient solves
 call the native forward and adjoint directly from the slot's thread
 (``solver.misfit_gradient``), so they do not queue behind PyTorch's single
 per-device autograd thread.  They keep one-byte INT8 histories with per-tile scales

@@ -93,7 +93,7 @@ class SolverConfig:
     region: str
     acc64: bool = True
     tm2d: bool = False
-    chunk: int = 16                                     # time steps per captured graph
+    chunk: int = 32                                     # time steps per captured graph
     tuning: Tuple[int, int, int, int] = (0, 0, 0, -1)   # dgb_set_tuning (see deepgpr_b200.autotune)
 
     @property
