@@ -139,6 +139,9 @@ struct StreamSet {
   // side stream: 2D TM frame kernels run on it beside the interior kernels
   cudaStream_t side = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
+  // second side stream: the imaging kernel beside the adjoint E step
+  cudaStream_t side2 = nullptr;
+  cudaEvent_t fork2 = nullptr, join2 = nullptr;
 };
 thread_local std::vector<StreamSet> g_streams;
 
@@ -179,6 +182,9 @@ StreamSet* stream_set() {
   if (cudaStreamCreateWithFlags(&s.side, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
   if (cudaEventCreateWithFlags(&s.fork, cudaEventDisableTiming) != cudaSuccess) return nullptr;
   if (cudaEventCreateWithFlags(&s.join, cudaEventDisableTiming) != cudaSuccess) return nullptr;
+  if (cudaStreamCreateWithFlags(&s.side2, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
+  if (cudaEventCreateWithFlags(&s.fork2, cudaEventDisableTiming) != cudaSuccess) return nullptr;
+  if (cudaEventCreateWithFlags(&s.join2, cudaEventDisableTiming) != cudaSuccess) return nullptr;
   g_streams.push_back(s);
   return &g_streams.back();
 }
@@ -2254,18 +2260,31 @@ void backward_impl(const BackwardCall<T>& bc) {
       auto issue = [&](int k) {
         TiledAdj<T> b = P;
         b.a.k_in_chunk = k;
-        if (want_model && img_blocks > 0) {
+        // The imaging of step it reads lambda_E (which the adjoint E step only
+        // reads) and the history, and writes the gradient sums: outside kernel
+        // timing it runs on the second side stream beside the adjoint E step,
+        // and the adjoint H step (which writes lambda_E) waits for it.
+        const bool img = want_model && img_blocks > 0;
+        const bool img_side = img && !g_prof.on && ss != nullptr && ss->side2 != nullptr;
+        cudaStream_t ist = st;
+        if (img_side) {
+          cudaEventRecord(ss->fork2, st);
+          cudaStreamWaitEvent(ss->side2, ss->fork2, 0);
+          ist = ss->side2;
+        }
+        if (img) {
           if (tm2d)
-            timed(KK_IMAGE, st, [&] { launch_tm_image<T>(kind, a.e_only != 0, a.acc64 != 0, st, b.a, tl.Ez, tg); });
+            timed(KK_IMAGE, st, [&] { launch_tm_image<T>(kind, a.e_only != 0, a.acc64 != 0, ist, b.a, tl.Ez, tg); });
           else
             timed(KK_IMAGE, st, [&] {
               const long long ls = (long long)g.NX * g.NY * kg.zp;
               if (a.box.cells() < (1LL << 31))
-                launch_k3_image<T>(kind, a.e_only != 0, a.acc64 != 0, cm.mode, st, b.a, kb, ls, g.NY * kg.zp, kg.zp);
+                launch_k3_image<T>(kind, a.e_only != 0, a.acc64 != 0, cm.mode, ist, b.a, kb, ls, g.NY * kg.zp, kg.zp);
               else
-                k_image<T><<<img_blocks, 256, 0, st>>>(b.a, kb.Ex, kb.Ey, kb.Ez, ls, g.NY * kg.zp, kg.zp);
+                k_image<T><<<img_blocks, 256, 0, ist>>>(b.a, kb.Ex, kb.Ey, kb.Ez, ls, g.NY * kg.zp, kg.zp);
             });
         }
+        if (img_side) cudaEventRecord(ss->join2, ss->side2);
         if (tm2d) {
           timed(KK_ADJ_E, st, [&] {
             return tm_launch(
@@ -2288,6 +2307,7 @@ void backward_impl(const BackwardCall<T>& bc) {
                   else tmi_adj_e<T, 4><<<gi, wblock, 0, q>>>(b, tl, pE.interior);
                 });
           });
+          if (img_side) cudaStreamWaitEvent(st, ss->join2, 0);   // the imaging read lambda_E
           timed(KK_ADJ_H, st, [&] {
             return tm_launch(
                 st, ss, pH,
@@ -2330,6 +2350,7 @@ void backward_impl(const BackwardCall<T>& bc) {
             if (zpass) k3p_adj_w<T, false><<<gph, kBlock, 0, st>>>(b, kb, kg, fh);
             return zpass ? 2 : 1;
           });
+          if (img_side) cudaStreamWaitEvent(st, ss->join2, 0);   // the imaging read lambda_E
           timed(KK_ADJ_H, st, [&] {
             if constexpr (sizeof(T) == 4) {
               if (wide3) k3w_adj_launch<1>(R, eq3, st, b, kb, kwg);
