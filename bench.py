@@ -26,9 +26,12 @@ cell-update.
 "serving" (also in the line; ``--only-serving`` prints it alone): a seeded
 Poisson stream with config 4's request mix (nt scaled by 0.1, 40 requests,
 all arriving within ~0.6 s so both paths run at capacity) served by
-``deepgpr_b200.serving.SolveServer`` (8 slots, INT8 histories) and, for
-comparison, by plain per-request ``compute`` (+ ``backward``) calls one after
-another (FP32 histories); solves/s and p50/p99 latency of both.
+``deepgpr_b200.serving.SolveServer`` (8 slots; FP32 histories, and again with
+INT8 one-byte histories) and, for comparison, by plain per-request
+``compute`` (+ ``backward``) calls one after another (FP32 histories; with the
+library's default memory policy and with the server's); solves/s and p50/p99
+latency of every arm, and the relative L2 error of every arm's gradients
+against an FP64 solve of each gradient request of the stream.
 
 ``--impl reference`` times the reference's own C/OpenMP CPU backend
 (oracle/_ref, compiled from the reference source) on a bounded sample of the
@@ -73,6 +76,8 @@ def parse():
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--only-serving", action="store_true", help="print the serving object alone")
     ap.add_argument("--serving-requests", type=int, default=40)
+    ap.add_argument("--serving-history", default="fp32", choices=("int8", "fp8", "bf16", "fp32"),
+                    help="history format of the served arm")
     ap.add_argument("--cpu-sample", action="store_true", help="time the CPU backend sample alone (internal)")
     ap.add_argument("--config3", action="store_true",
                     help="3D order-8 gradient of the 200^3 config (8 shots, nt 2500, BF16 E+R history) with "
@@ -320,7 +325,7 @@ def ours(args, rank, world, local):
         # a serving process runs with PyTorch's stream-ordered allocator (see deepgpr_b200.serving)
         env = dict(os.environ, PYTORCH_CUDA_ALLOC_CONF="backend:cudaMallocAsync")
         cmd = [sys.executable, str(Path(__file__).resolve()), "--only-serving",
-               "--serving-requests", str(args.serving_requests)]
+               "--serving-requests", str(args.serving_requests), "--serving-history", args.serving_history]
         proc = subprocess.run(cmd, env=env, capture_output=True, text=True)
         try:
             serving = json.loads(proc.stdout.strip().splitlines()[-1])
@@ -466,8 +471,17 @@ def config3_measure(dev, nt=2500, steps=1):
     }
 
 
-def serving_measure(dev, n=40, slots=8):
-    """Config-4 stream: continuous-batching server (INT8 histories) vs plain per-request launches (FP32)."""
+def serving_measure(dev, n=40, slots=8, history="fp32"):
+    """Config-4 stream: continuous-batching server vs plain per-request launches.
+
+    Arms, in this order: plain per-request ``compute`` (+ ``backward``) calls
+    with the library's default memory policy; the same with the server's
+    policy (freed memory kept mapped in the stream-ordered pool, so pool
+    unmapping at synchronisations does not enter the comparison); the server
+    with ``history`` histories; the server with INT8 one-byte histories.  Every
+    gradient of every arm is compared with an FP64 solve of the same request.
+    """
+    from deepgpr_b200 import native
     from deepgpr_b200.serving import SolveServer, percentile, run_plain
     from deepgpr_b200.synthetic import serving_stream
 
@@ -475,20 +489,30 @@ def serving_measure(dev, n=40, slots=8):
     warm, _ = serving_stream(seed=7, n=4, nt_scale=0.02)
     run_plain(warm, dev)                                   # load, first-call set-up
     torch.cuda.synchronize()
+    plain_default = run_plain(reqs, dev, arrivals=arrivals, history="fp32")
+    torch.cuda.synchronize()
+    free, _ = torch.cuda.mem_get_info(dev)
+    native.set_scratch_retention(int(0.8 * free))
     plain = run_plain(reqs, dev, arrivals=arrivals, history="fp32")
     torch.cuda.synchronize()
-    with SolveServer(dev, slots=slots, history="int8") as srv:
-        for f in [srv.submit(r) for r in warm]:
-            f.result()
-        t0 = time.perf_counter()
-        futs = []
-        for req, at in zip(reqs, arrivals):
-            wait = at - (time.perf_counter() - t0)
-            if wait > 0:
-                time.sleep(wait)
-            futs.append(srv.submit(req))
-        served = [f.result() for f in futs]
-        peak_running, peak_reserved = srv.peak_running, srv.peak_reserved
+    native.set_scratch_retention(0)
+
+    def serve(fmt):
+        with SolveServer(dev, slots=slots, history=fmt) as srv:
+            for f in [srv.submit(r) for r in warm]:
+                f.result()
+            t0 = time.perf_counter()
+            futs = []
+            for req, at in zip(reqs, arrivals):
+                wait = at - (time.perf_counter() - t0)
+                if wait > 0:
+                    time.sleep(wait)
+                futs.append(srv.submit(req))
+            out = [f.result() for f in futs]
+            return out, srv.peak_running, srv.peak_reserved
+
+    served, peak_running, peak_reserved = serve(history)
+    served_i8, peak_running_i8, peak_reserved_i8 = serve("int8")
 
     def summary(res):
         span = max(r.finished for r in res) - min(r.submitted for r in res)
@@ -496,18 +520,77 @@ def serving_measure(dev, n=40, slots=8):
         return {"solves_per_s": len(res) / span, "p50_latency_s": percentile(lat, 50),
                 "p99_latency_s": percentile(lat, 99), "span_s": span}
 
-    sp, ss = summary(plain), summary(served)
+    sp, sd, ss, si = summary(plain), summary(plain_default), summary(served), summary(served_i8)
     kinds = {k: sum(r.kind == k for r in reqs) for k in ("forward", "gradient")}
+    arms = {"plain_fp32": plain, f"served_{history}": served}
+    if history != "int8":
+        arms["served_int8"] = served_i8
+    error = served_gradient_error(reqs, arms, dev)
+    plain_path = "compute (+ backward) per request, one after another"
     return {
         "workload": "config-4 request mix (2D forward 128^2-1024^2 x 1-16 shots, order 2/4; 3D gradient "
                     "96^3-160^3 x 1-4 shots, order 4), seeded Poisson arrivals",
         "sample": f"{n} requests ({kinds['forward']} forward, {kinds['gradient']} gradient), nt scaled by 0.1, "
                   f"arrivals within {arrivals[-1]:.2f} s",
-        "plain": dict(sp, history="fp32", path="compute (+ backward) per request, one after another"),
-        "served": dict(ss, history="int8", slots=slots, peak_running=peak_running,
+        "plain": dict(sp, history="fp32", path=plain_path,
+                      memory="freed memory kept mapped, as in the server"),
+        "plain_default_pool": dict(sd, history="fp32", path=plain_path,
+                                   memory="library default (pool trimmed at synchronisations)"),
+        "served": dict(ss, history=history, slots=slots, peak_running=peak_running,
                        peak_reserved_gib=round(peak_reserved / 2**30, 2)),
+        "served_int8": dict(si, history="int8", slots=slots, peak_running=peak_running_i8,
+                            peak_reserved_gib=round(peak_reserved_i8 / 2**30, 2)),
         "speedup_solves_per_s": ss["solves_per_s"] / sp["solves_per_s"],
+        "speedup_int8_solves_per_s": si["solves_per_s"] / sp["solves_per_s"],
+        "speedup_vs_default_pool": ss["solves_per_s"] / sd["solves_per_s"],
+        "gradient_error_vs_fp64": error,
     }
+
+
+def served_gradient_error(reqs, arms, dev, budget_bytes=40 * 2**30):
+    """Relative L2 error of each arm's gradients (``arms``: name -> results in
+    request order) against an FP64 solve of each gradient request.
+
+    Requests whose FP64 history would exceed ``budget_bytes`` are skipped."""
+    import deepgpr_b200 as dg
+
+    def rel(a, b):
+        b = b.double().cpu()
+        return float((a.double().cpu() - b).norm() / b.norm())
+
+    errs = {name: ([], []) for name in arms}
+    skipped = 0
+    for n, req in enumerate(reqs):
+        if req.kind != "gradient":
+            continue
+        pml = req.pmlthick if isinstance(req.pmlthick, int) else max(req.pmlthick)
+        cells = 1
+        for m in req.eps_r.shape:
+            cells *= m + 2 * pml + 1
+        comps = 3 if req.mode == 3 else 1
+        if cells * req.source_location.shape[0] * req.source_amplitudes.shape[-1] * 8 * comps > budget_bytes:
+            skipped += 1
+            continue
+        f64 = torch.float64
+        eps = req.eps_r.to(dev, f64).requires_grad_(True)
+        sig = req.sigma.to(dev, f64).requires_grad_(True)
+        rx = dg.compute(dev, eps_r=eps, sigma=sig, source_amplitudes=req.source_amplitudes.to(dev, f64),
+                        source_location=req.source_location.to(dev), receiver_location=req.receiver_location.to(dev),
+                        dx=req.dx, dt=req.dt, pmlthick=req.pmlthick, fdtd_order=req.fdtd_order, mode=req.mode,
+                        precision=f64)[-1]
+        (0.5 * ((rx - req.observed.to(dev, f64)) ** 2).sum()).backward()
+        for name, res in arms.items():
+            errs[name][0].append(rel(res[n].grad_eps_r, eps.grad))
+            errs[name][1].append(rel(res[n].grad_sigma, sig.grad))
+        del eps, sig, rx
+        torch.cuda.empty_cache()
+    out = {"requests": len(next(iter(errs.values()))[0]), "skipped": skipped,
+           "oracle": "FP64 run of the same request"}
+    for name, (e, s) in errs.items():
+        if e:
+            out[name] = {"eps_r_max": max(e), "sigma_max": max(s), "eps_r_median": statistics.median(e),
+                         "sigma_median": statistics.median(s)}
+    return out
 
 
 def host_cpu():
@@ -612,7 +695,8 @@ def main():
                 print(json.dumps(config3_measure(torch.device("cuda", local), nt=args.config3_nt)), flush=True)
         elif args.only_serving:
             if rank == 0:
-                print(json.dumps(serving_measure(torch.device("cuda", local), n=args.serving_requests)), flush=True)
+                print(json.dumps(serving_measure(torch.device("cuda", local), n=args.serving_requests,
+                                                 history=args.serving_history)), flush=True)
         elif args.only_3d:
             if rank == 0:
                 shape = tuple(int(v) for v in args.shape_3d.split(","))

@@ -32,6 +32,7 @@ def test_footprint_grows_with_work_and_fp8_is_smaller():
     assert footprint_bytes(_req("d", "forward", nt=100)) < small
     big = _req("e", "gradient", shape=(100, 100, 100), nt=500)
     assert footprint_bytes(big, "fp8") < footprint_bytes(big, "fp32")
+    assert footprint_bytes(big, "int8") < footprint_bytes(big, "bf16") <= footprint_bytes(big, "fp32")
 
 
 def test_percentile_nearest_rank():
@@ -176,7 +177,7 @@ def test_direct_gradient_equals_compute_backward(dims, cuda_device):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("history", ["int8", "fp8", "fp32"])
+@pytest.mark.parametrize("history", ["bf16", "int8", "fp8", "fp32"])
 def test_results_are_the_same_alone_and_in_the_mix(history, cuda_device):
     reqs = [_problem(2, "forward", 0, nt=80, shots=2), _problem(2, "gradient", 1, nt=80, shots=2),
             _problem(3, "gradient", 2, nt=40), _problem(3, "forward", 3, nt=40, shots=2),
@@ -194,10 +195,10 @@ def test_results_are_the_same_alone_and_in_the_mix(history, cuda_device):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("history", ["fp8", "int8"])
+@pytest.mark.parametrize("history", ["fp8", "int8", "bf16"])
 @pytest.mark.parametrize("dims", [2, 3])
 def test_served_one_byte_gradient_error_against_fp64(dims, history, cuda_device):
-    """Served one-byte-history gradient against an FP64 run of the same request (bounds written here)."""
+    """Served compressed-history gradient against an FP64 run of the same request (bounds written here)."""
     import deepgpr_b200 as dg
     from helpers import rel_l2
 
@@ -218,5 +219,5 @@ def test_served_one_byte_gradient_error_against_fp64(dims, history, cuda_device)
     print(f"{history} vs fp64 ({dims}D): grad_eps {e_eps:.3e}, grad_sigma {e_sig:.3e}")
     # measured on B200 (eps_r / sigma): FP8 2D 5.0e-3 / 5.4e-3, 3D 5.0e-3 / 7.0e-3;
     # INT8 2D 1.35e-3 / 9.1e-4, 3D 1.18e-3 / 7.0e-4
-    bound = 1e-2 if history == "fp8" else 2e-3
+    bound = {"fp8": 1e-2, "int8": 2e-3, "bf16": 1e-3}[history]
     assert e_eps < bound and e_sig < bound
