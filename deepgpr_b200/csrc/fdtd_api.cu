@@ -847,7 +847,12 @@ bool k3_cpml_single(const Grid& g, const int* p) {
   return true;
 }
 
-K3Geom k3_layout(const Grid& g) {
+// min_chunks: the fewest x chunks to use (capped at chunks of 16 planes).
+// Measured on 320 x 320 x 160, 200^3 and 160^3 + CPML 10 (4 shots): the
+// z-streamed adjoint steps are fastest at about 8 chunks (4-6 % faster than
+// the wave-fill choice below, which assumes the forward kernels' residency),
+// the z-streamed H step at about 12 (5-8 % faster).
+K3Geom k3_layout(const Grid& g, int min_chunks) {
   K3Geom kg;
   memset(&kg, 0, sizeof(kg));
   kg.zp = (g.NZ + 31) / 32 * 32;
@@ -875,6 +880,7 @@ K3Geom k3_layout(const Grid& g) {
       best = n;
     }
   }
+  best = std::max(best, std::min(min_chunks, std::max(1, g.NX / 16)));
   if (g_opt.k3_xchunks > 0) best = std::min(g_opt.k3_xchunks, g.NX);
   kg.xc = (g.NX + best - 1) / best;
   kg.nchunk = (g.NX + kg.xc - 1) / kg.xc;
@@ -1263,19 +1269,25 @@ double k3_interior_fraction(const Grid& g, const int* p) {
 }
 
 // Automatic family of a half step (FP32, wide kernels usable).  The wide
-// kernels need busy lanes: at least 70 % of their 128-column strips' lanes
-// hold grid columns (the z-streamed kernels use 64-column strips).  Then the
-// wide E forward step of the pass form is taken always, and the wide H
+// kernels need busy lanes: the share of their 128-column strips' lanes that
+// hold grid columns (the z-streamed kernels use 64-column strips).  The wide
+// E forward step of the pass form is taken at 70 % busy lanes; the wide H
 // forward step, E forward step with its CPML in the kernel and adjoint steps
-// when at least 3/4 of the cells lie outside the CPML frame.  Measured with
-// the z-streamed kernels as the alternative: on 320 x 320 x 160 + CPML 10
-// (77 % outside, 71 % busy lanes) the wide kernels are 2-10 % faster per
-// half step; on 160 x 160 x 96 + CPML 10 (65 %, 91 %) the wide E pass-form
-// step is 17 % faster and the others 8-34 % slower (they read the x- and
-// y-face CPML operands where they are used); on 140^3 + CPML 10 (64 %, 63 %)
-// the wide E pass-form step is 6 % slower.
+// at 80 % busy lanes with at least 70 % of the cells outside the CPML frame.
+// Measured against the z-streamed kernels, both at their best x chunks
+// (k3_layout, k3w_layout): on 320 x 320 x 160 + CPML 10 (77 % outside, 71 %
+// busy lanes) the wide E pass-form step is 11 % faster, the z-streamed H
+// step 2 % and the z-streamed adjoint steps 10-11 % faster; on 200^3 + CPML
+// 10 (74 %, 86 %) the wide H and adjoint steps are 10 % and 6-8 % faster; on
+// 160^3 + CPML 10 (69 %, 71 %) the wide E pass-form step is 10 % faster and
+// the wide adjoint steps 15 % slower; on 160 x 160 x 96 + CPML 10 (65 %,
+// 91 %) the wide E pass-form step is 17 % faster and the others 8-34 %
+// slower (they read the x- and y-face CPML operands where they are used);
+// on 140^3 + CPML 10 (64 %, 63 %) the wide E pass-form step is 6 % slower.
 double k3w_lane_use(const Grid& g) { return (double)g.NZ / (double)(((g.NZ + 31) / 32 * 32 + KWW - 1) / KWW * KWW); }
-bool k3w_auto(bool e_pass, double interior, double lanes) { return lanes >= 0.7 && (e_pass || interior >= 0.75); }
+bool k3w_auto(bool e_pass, double interior, double lanes) {
+  return e_pass ? lanes >= 0.7 : (lanes >= 0.8 && interior >= 0.7);
+}
 
 // Whether the wide kernels take a 3D FP32 forward solve: radius <= 2, the
 // single-face CPML form (or none) and at most 64 z-face cells of E and of H
@@ -1368,7 +1380,9 @@ void k3w_adj_launch(int R, bool eq, cudaStream_t st, const TiledAdj<float>& P, c
   }
 }
 
-K3WGeom k3w_layout(const Grid& g, int zp) {
+// min_chunks as in k3_layout (the wide adjoint steps: 12 measured 2-3 %
+// faster than the wave-fill choice on 320 x 320 x 160 + CPML 10).
+K3WGeom k3w_layout(const Grid& g, int zp, int min_chunks) {
   K3WGeom kg;
   memset(&kg, 0, sizeof(kg));
   kg.zp = zp;
@@ -1382,7 +1396,8 @@ K3WGeom k3w_layout(const Grid& g, int zp) {
     blocks = KW_MIN_BLOCKS;
   }
   const long long per = (long long)g.nshot * kg.nzs * kg.nyt;
-  const int n = k3_pick_xchunks(g.NX, per, (double)sm_count() * blocks, 3.0);
+  int n = k3_pick_xchunks(g.NX, per, (double)sm_count() * blocks, 3.0);
+  if (g_opt.k3_xchunks <= 0) n = std::max(n, std::min(min_chunks, std::max(1, g.NX / 16)));
   kg.xc = (g.NX + n - 1) / n;
   kg.nchunk = (g.NX + kg.xc - 1) / kg.xc;
   kg.nblocks = per * kg.nchunk;
@@ -1702,7 +1717,7 @@ void forward_impl(const ForwardCall<T>& fc) {
     const int cpm_h = cpm_base;
     const int cpm_e = (pass3 && !keep_r) ? kCpmPass : cpm_base;
     if (ok && !tm2d) {
-      kg = k3_layout(g);
+      kg = k3_layout(g, 12);
       kg.src_rows = src_rows;
       kg.rcv_rows = rcv_rows;
       kg.cpml_single = k3_cpml_single(g, cm.p);
@@ -1723,7 +1738,7 @@ void forward_impl(const ForwardCall<T>& fc) {
     K3WGeom kwg;
     memset(&kwg, 0, sizeof(kwg));
     if (wideH || wideE) {
-      kwg = k3w_layout(g, kg.zp);
+      kwg = k3w_layout(g, kg.zp, 0);
       kwg.src_rows = src_rows;
       kwg.rcv_rows = rcv_rows;
       for (int ax = 0; ax < 3; ++ax) {
@@ -2187,7 +2202,7 @@ void backward_impl(const BackwardCall<T>& bc) {
     K3Buf<T> kb;
     memset(&kb, 0, sizeof(kb));
     if (ok && !tm2d) {
-      kg = k3_layout(g);
+      kg = k3_layout(g, 8);
       kg.src_rows = src_rows;
       kg.rcv_rows = rcv_rows;
       kg.cpml_single = k3_cpml_single(g, cm.p);
@@ -2205,7 +2220,7 @@ void backward_impl(const BackwardCall<T>& bc) {
     K3WGeom kwg;
     memset(&kwg, 0, sizeof(kwg));
     if (wide3) {
-      kwg = k3w_layout(g, kg.zp);
+      kwg = k3w_layout(g, kg.zp, 12);
       kwg.src_rows = src_rows;
       kwg.rcv_rows = rcv_rows;
     }
