@@ -1180,9 +1180,12 @@ __global__ void __launch_bounds__(kBlock) k3p_fwd_e(TiledFwd<T> P, K3Buf<T> f, K
   qf[4] = k > 0 ? q_low_e(a.eF[4].p, k) : -1;
   qf[5] = k > 0 ? q_high(a.eF[5].p, k, g.NZ) : -1;
   const bool any_pml = qf[0] >= 0 || qf[1] >= 0 || qf[2] >= 0 || qf[3] >= 0 || qf[4] >= 0 || qf[5] >= 0;
-  const bool pts = (kg.src_rows && kg.src_rows[(long long)s * g.NX + i]) ||
-                   (kg.rcv_rows && kg.rcv_rows[(long long)s * g.NX + i]);
-  if (!(any_pml || pts)) return;
+  // the plane's point flags are loaded here and read after the corrections:
+  // a CPML cell (nearly every frame cell) does not wait for them
+  const unsigned char fsrc = kg.src_rows ? kg.src_rows[(long long)s * g.NX + i] : (unsigned char)0;
+  const unsigned char frcv = kg.rcv_rows ? kg.rcv_rows[(long long)s * g.NX + i] : (unsigned char)0;
+  if (!any_pml && (fsrc | frcv) == 0) return;
+  const bool pts = (fsrc | frcv) != 0;
   const int cc = i * PS + j * zp + k;
   const long long base = (long long)s * g.NX * PS + cc;
   const T cb = f.ce_rhs[cc];

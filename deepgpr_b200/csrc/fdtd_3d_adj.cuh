@@ -1156,7 +1156,9 @@ __global__ void __launch_bounds__(kBlock) k3p_adj_w(const __grid_constant__ Tile
                                                     K3Faces fs) {
   const AdjArgs<T>& a = P.a;
   const Grid& g = a.g;
-  if (EF && a.ctrl->cur - a.k_in_chunk - 1 < 0) return;   // no head after the last reverse step
+  // no head after the last reverse step: read here, checked before the stores,
+  // so the cell's loads do not wait for the step counter
+  const bool head = !EF || a.ctrl->cur - a.k_in_chunk - 1 >= 0;
   const unsigned t = blockIdx.x * kBlock + threadIdx.x;
   if (t >= fs.cum[5]) return;
   int b = 0;
@@ -1201,13 +1203,28 @@ __global__ void __launch_bounds__(kBlock) k3p_adj_w(const __grid_constant__ Tile
     on2 = axis == 2 ? jl : kl;
     sg1 = axis == 1 ? T(1) : T(-1);
   }
+  T w1 = T(0), w2 = T(0), p1 = T(0), p2 = T(0);
+  int pi1 = 0, pi2 = 0;
   if (on1) {
-    const int pi = cpml_at32<EF>(g, axis, 1, F.p, s, q, i, j, k);
-    F.w1[pi] = pml_weight_v(l1[base], inv, up, sg1, pr, F.psi1[pi], &F.psi1[pi]);
+    pi1 = cpml_at32<EF>(g, axis, 1, F.p, s, q, i, j, k);
+    const T lam = l1[base], ph = F.psi1[pi1];
+    w1 = (sg1 * up * pr.ra1 * lam - pr.rf * ph) * inv;   // pml_weight_v, the stores below
+    p1 = sg1 * up * pr.rb * lam + pr.re * ph;
   }
   if (on2) {
-    const int pi = cpml_at32<EF>(g, axis, 2, F.p, s, q, i, j, k);
-    F.w2[pi] = pml_weight_v(l2[base], inv, up, -sg1, pr, F.psi2[pi], &F.psi2[pi]);
+    pi2 = cpml_at32<EF>(g, axis, 2, F.p, s, q, i, j, k);
+    const T lam = l2[base], ph = F.psi2[pi2], sg2 = -sg1;
+    w2 = (sg2 * up * pr.ra1 * lam - pr.rf * ph) * inv;
+    p2 = sg2 * up * pr.rb * lam + pr.re * ph;
+  }
+  if (!head) return;
+  if (on1) {
+    F.w1[pi1] = w1;
+    F.psi1[pi1] = p1;
+  }
+  if (on2) {
+    F.w2[pi2] = w2;
+    F.psi2[pi2] = p2;
   }
 }
 
