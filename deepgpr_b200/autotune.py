@@ -47,7 +47,7 @@ def search_space(cfg) -> List[Tuple[str, Sequence[int]]]:
     """Coordinates searched in turn (the first value of each is the default)."""
     if cfg.tm2d:
         return [("tm_chunks", (0, 1, 2, 4, 8)), ("tm_frame_rows", (0, 4, 8, 32)), ("chunk", (32, 16, 64))]
-    space: List[Tuple[str, Sequence[int]]] = [("k3_xchunks", (0, 1, 2, 4, 8, 16))]
+    space: List[Tuple[str, Sequence[int]]] = [("k3_xchunks", (0, 4, 8, 12, 16, 24))]
     if cfg.dtype == torch.float32:
         space.append(("tma", (2, 0, 1)))
     space.append(("chunk", (32, 16, 64)))
