@@ -1088,9 +1088,14 @@ __global__ void __launch_bounds__(32 * K3_WARPS, k3_min_blocks<T, R>()) k3v_fwd_
 // (NX * ceil(NY / kZfRowsF), nshot).
 // ---------------------------------------------------------------------------
 constexpr int kZfRowsF = 8;
+// Resident CTAs per SM of the forward CPML passes (k3z_fwd_h, k3p_fwd_e):
+// latency-bound per-cell work, so residency counts more than registers
+// (8: 32 registers a thread; measured on 320 x 320 x 160 + CPML 10 the E
+// half step 7 % and the H half step 3 % faster than at 44-47 registers).
+constexpr int kPassMinBlocks = 8;
 
 template <typename T, int R>
-__global__ void __launch_bounds__(32 * kZfRowsF) k3z_fwd_h(TiledFwd<T> P, K3Buf<T> f, K3Geom kg, int nyb) {
+__global__ void __launch_bounds__(32 * kZfRowsF, kPassMinBlocks) k3z_fwd_h(TiledFwd<T> P, K3Buf<T> f, K3Geom kg, int nyb) {
   const FwdArgs<T>& a = P.a;
   const Grid& g = a.g;
   const int NX = g.NX, NY = g.NY, NZ = g.NZ;
@@ -1165,7 +1170,7 @@ __device__ __forceinline__ bool k3_frame_cell(const K3Frame& fr, unsigned t, int
 }
 
 template <typename T, int R>
-__global__ void __launch_bounds__(kBlock) k3p_fwd_e(TiledFwd<T> P, K3Buf<T> f, K3Geom kg) {
+__global__ void __launch_bounds__(kBlock, kPassMinBlocks) k3p_fwd_e(TiledFwd<T> P, K3Buf<T> f, K3Geom kg) {
   const FwdArgs<T>& a = P.a;
   const Grid& g = a.g;
   int i, j, k;
