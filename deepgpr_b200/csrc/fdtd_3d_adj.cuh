@@ -1002,9 +1002,13 @@ __global__ void __launch_bounds__(32 * K3_WARPS) k3v_adj_head(TiledAdj<T> P, K3B
 // s * ls + i * lp + j * lr + k.
 // ---------------------------------------------------------------------------
 constexpr int kImage3Threads = 128;
+// Resident CTAs per SM of k3_image: 8 (64 registers a thread) measured 6 %
+// faster than 80 registers on 320 x 320 x 160 and 160^3 + CPML 10 (4 shots);
+// 12 (40 registers) spills and is 17 % slower.
+constexpr int kImage3MinBlocks = 8;
 
 template <typename T, int KIND, bool EONLY, bool ACC64, int NC>
-__global__ void __launch_bounds__(kImage3Threads) k3_image(AdjArgs<T> a, const T* __restrict__ lx,
+__global__ void __launch_bounds__(kImage3Threads, kImage3MinBlocks) k3_image(AdjArgs<T> a, const T* __restrict__ lx,
                                                            const T* __restrict__ ly, const T* __restrict__ lz,
                                                            long long ls, int lp, int lr) {
   constexpr int U = NC == 1 ? 4 : 2;
