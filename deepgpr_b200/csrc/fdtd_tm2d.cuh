@@ -1320,9 +1320,14 @@ __device__ __forceinline__ void tmi_adj_h_run(const TiledAdj<T>& P, const TmBuf<
   }
 }
 
+// Resident CTAs per SM of the interior kernels: 6 (80 registers a thread)
+// measured 1 % faster per config-2 gradient than the unconstrained build
+// (93-126 registers); 8 (64 registers) spills and is 15 % slower.
+constexpr int kTmiMinBlocks = 6;
+
 #define DG_TMI_WRAPPER(NAME, ARGS, BUF)                                                               \
   template <typename T, int R>                                                                       \
-  __global__ void __launch_bounds__(32 * TM_WARPS) NAME(ARGS<T> P, TmBuf<T> t, TmGeom tg) {          \
+  __global__ void __launch_bounds__(32 * TM_WARPS, kTmiMinBlocks) NAME(ARGS<T> P, TmBuf<T> t, TmGeom tg) { \
     NAME##_run<T, R>(P, t, tg, blockIdx.x);                                                          \
   }
 DG_TMI_WRAPPER(tmi_fwd_h, TiledFwd, f)
