@@ -98,3 +98,15 @@ def test_options_validation(lib):
 def test_marshal_rejects_missing_and_unknown_names():
     with pytest.raises(KeyError):
         native.marshal(native.FORWARD_SIGNATURE, {"dt": 1.0})
+
+
+def test_build_recipe_compiles_the_device_code_as_one_unit():
+    """Split compilation optimises groups of device functions separately and the
+    grouping follows the whole translation unit: an edit of host code alone
+    changed kernels' registers and speed.  The recipe must not ask for it, and
+    must keep strict IEEE single precision (the reference's rounding)."""
+    from deepgpr_b200 import build
+
+    assert not any(flag.startswith("-split-compile") for flag in build.NVCC_FLAGS)
+    assert "-fmad=false" in build.NVCC_FLAGS
+    assert "arch=compute_100a,code=sm_100a" in build.NVCC_FLAGS
