@@ -75,23 +75,26 @@ struct K3Geom {
   int zpost_h;                     // H z-face corrections in k3z_fwd_h after k3v_fwd_h
 };
 
-// (rows, n) <-> (rows, pitch) with zero padding.
+// (rows, n) <-> (rows, pitch) with zero padding: one warp per row, lanes over
+// the columns (no integer division per element).
 template <typename T>
 __global__ void k_pack_rows(const T* __restrict__ src, T* __restrict__ dst, long long rows, int n, int pitch) {
-  const long long tot = rows * pitch;
-  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < tot; w += (long long)gridDim.x * blockDim.x) {
-    const long long r = w / pitch;
-    const int c = int(w - r * pitch);
-    dst[w] = c < n ? src[r * n + c] : T(0);
+  const int lane = threadIdx.x & 31;
+  const long long nw = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long r = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5); r < rows; r += nw) {
+    const T* __restrict__ s = src + r * n;
+    T* __restrict__ d = dst + r * pitch;
+    for (int c = lane; c < pitch; c += 32) d[c] = c < n ? s[c] : T(0);
   }
 }
 template <typename T>
 __global__ void k_unpack_rows(const T* __restrict__ src, T* __restrict__ dst, long long rows, int n, int pitch) {
-  const long long tot = rows * n;
-  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < tot; w += (long long)gridDim.x * blockDim.x) {
-    const long long r = w / n;
-    const int c = int(w - r * n);
-    dst[w] = src[r * pitch + c];
+  const int lane = threadIdx.x & 31;
+  const long long nw = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long r = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5); r < rows; r += nw) {
+    const T* __restrict__ s = src + r * pitch;
+    T* __restrict__ d = dst + r * n;
+    for (int c = lane; c < n; c += 32) d[c] = s[c];
   }
 }
 

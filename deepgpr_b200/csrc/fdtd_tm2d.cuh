@@ -1391,11 +1391,12 @@ __global__ void __launch_bounds__(32 * TM_WARPS) tmf_adj_h(TiledAdj<T> P, TmBuf<
 // (nshot, NX, NY, 2) plane k = 0  <->  (nshot, NX, NYP) with zero padding.
 template <typename T>
 __global__ void k_pack2d_pitch(const T* __restrict__ src, T* __restrict__ dst, long long rows, int NY, int NYP) {
-  const long long n = rows * NYP;
-  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < n; w += (long long)gridDim.x * blockDim.x) {
-    const long long r = w / NYP;
-    const int j = int(w % NYP);
-    dst[w] = j < NY ? src[2 * (r * NY + j)] : T(0);
+  const int lane = threadIdx.x & 31;
+  const long long nw = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long r = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5); r < rows; r += nw) {
+    const T* __restrict__ s = src + 2 * (r * NY);
+    T* __restrict__ d = dst + r * NYP;
+    for (int j = lane; j < NYP; j += 32) d[j] = j < NY ? s[2 * j] : T(0);
   }
 }
 // As k_pack2d_pitch for a curl coefficient, scaled to the y difference:
@@ -1403,20 +1404,22 @@ __global__ void k_pack2d_pitch(const T* __restrict__ src, T* __restrict__ dst, l
 template <typename T>
 __global__ void k_pack2d_pitch_ys(const T* __restrict__ src, T* __restrict__ dst, long long rows, int NY, int NYP,
                                   T dx, T dy) {
-  const long long n = rows * NYP;
-  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < n; w += (long long)gridDim.x * blockDim.x) {
-    const long long r = w / NYP;
-    const int j = int(w % NYP);
-    dst[w] = j < NY ? src[2 * (r * NY + j)] * dx / dy : T(0);
+  const int lane = threadIdx.x & 31;
+  const long long nw = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long r = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5); r < rows; r += nw) {
+    const T* __restrict__ s = src + 2 * (r * NY);
+    T* __restrict__ d = dst + r * NYP;
+    for (int j = lane; j < NYP; j += 32) d[j] = j < NY ? s[2 * j] * dx / dy : T(0);
   }
 }
 template <typename T>
 __global__ void k_unpack2d_pitch(const T* __restrict__ src, T* __restrict__ dst, long long rows, int NY, int NYP) {
-  const long long n = rows * NY;
-  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < n; w += (long long)gridDim.x * blockDim.x) {
-    const long long r = w / NY;
-    const int j = int(w % NY);
-    dst[2 * w] = src[r * NYP + j];
+  const int lane = threadIdx.x & 31;
+  const long long nw = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long r = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5); r < rows; r += nw) {
+    const T* __restrict__ s = src + r * NYP;
+    T* __restrict__ d = dst + 2 * (r * NY);
+    for (int j = lane; j < NY; j += 32) d[2 * j] = s[j];
   }
 }
 
