@@ -35,6 +35,20 @@ def test_footprint_grows_with_work_and_fp8_is_smaller():
     assert footprint_bytes(big, "int8") < footprint_bytes(big, "bf16") <= footprint_bytes(big, "fp32")
 
 
+def test_history_formats_map_to_compute_options():
+    from deepgpr_b200.serving import HISTORY_FORMATS, history_options
+
+    assert history_options("fp32") == {"wavefield_compression": "none"}
+    assert history_options("bf16") == {"wavefield_compression": "none", "wavefield_storage_dtype": torch.bfloat16}
+    assert history_options("int8") == {"wavefield_compression": "int8"}
+    assert history_options("fp8") == {"wavefield_compression": "fp8"}
+    assert set(HISTORY_FORMATS) == {"fp32", "bf16", "int8", "fp8"}
+    with pytest.raises(ValueError):
+        history_options("fp16")
+    with pytest.raises(ValueError, match="history must be"):
+        SolveServer(slots=1, memory_budget=100, run=lambda r, s: None, history="fp16")
+
+
 def test_percentile_nearest_rank():
     v = [5.0, 1.0, 3.0, 2.0, 4.0]
     assert percentile(v, 50) == 3.0
