@@ -39,7 +39,18 @@ CASES = {
     "3d_o4_asym_pml": lambda: problem_3d(nt=20, order=4, pml=[3, 2, 4, 1, 2, 3], want_source=True),
     "3d_o8_stored": lambda: problem_3d(nt=15, order=8, shape=(18, 16, 14), pml=4, rhs_from_e=False),
     "3d_aniso": lambda: problem_3d(nt=15, order=4, dx=(0.02, 0.017, 0.013), dt=1e-11),
+    "3d_bf16_stored_S2": lambda: problem_3d(nt=16, order=4, storage_kind=2, rhs_from_e=False, interval=2),
+    "3d_f16_e_only": lambda: problem_3d(nt=16, order=2, storage_kind=1),
+    "3d_no_pml_physical": lambda: problem_3d(nt=12, order=4, pml=0, region="physical"),
+    "2d_two_shots_source_grad": lambda: _two_shots_2d(),
 }
+
+
+def _two_shots_2d():
+    p = problem_2d(nt=50, order=4, want_source=True)
+    p.source_location = torch.tensor([[[10, 10, 0]], [[20, 25, 0]]], dtype=torch.int32)
+    p.receiver_location = torch.tensor([[[10, 30, 0], [5, 7, 0]], [[25, 5, 0], [20, 25, 0]]], dtype=torch.int32)
+    return p
 
 
 @pytest.fixture(scope="module", autouse=True)
