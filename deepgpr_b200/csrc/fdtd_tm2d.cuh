@@ -1321,8 +1321,9 @@ __device__ __forceinline__ void tmi_adj_h_run(const TiledAdj<T>& P, const TmBuf<
 }
 
 // Resident CTAs per SM of the interior kernels: 6 (80 registers a thread)
-// measured 1 % faster per config-2 gradient than the unconstrained build
-// (93-126 registers); 8 (64 registers) spills and is 15 % slower.
+// measured 1 % faster per gradient of a 400 x 800 grid (32 shots, order 4)
+// than the unconstrained build (93-126 registers); 8 (64 registers) spills
+// and is 15 % slower.
 constexpr int kTmiMinBlocks = 6;
 
 #define DG_TMI_WRAPPER(NAME, ARGS, BUF)                                                               \

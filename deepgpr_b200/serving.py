@@ -24,9 +24,10 @@ call the native forward and adjoint directly from the slot's thread
 (``solver.misfit_gradient``), so they do not queue behind PyTorch's single
 per-device autograd thread.  They keep the exact FP32 E-only histories by
 default (``history="fp32"``).  ``history="bf16"`` keeps BF16 E and R (the
-same bytes as FP32 E alone; on config-4 style 3D gradient requests the
-eps_r gradient within 1e-3 of an FP64 solve, sigma within about 2e-3);
-``history="int8"`` stores one-byte INT8 codes with per-tile scales and
+same bytes as FP32 E alone; on 3D gradient requests of 96^3-160^3 cells,
+1-4 shots and 80-150 steps the eps_r gradient within 1e-3 of an FP64 solve,
+sigma within about 2e-3); ``history="int8"`` stores one-byte INT8 codes with
+per-tile scales and
 ``"fp8"`` E4M3 codes on the same tiles, which halve the history footprint at
 a gradient error of about 0.5-2 % on those requests (0.1-0.5 % on small
 test problems).
